@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark: Gcell-updates/s of one forward + adjoint gradient evaluation
+(128^3 model, 152^3 padded, 16 shots, nt = 2000; config 2).
+
+A step is one full gradient evaluation over the rank's 16 shots (forward
+with boundary-shell storage, misfit, reverse reconstruction + adjoint with
+imaging).  With N GPUs (torchrun, one process per GPU) every rank owns 16
+shots of a 16*N-shot survey (weak scaling) and the lambda/mu/rho gradients
+and the misfit are summed with one NCCL all-reduce per step.
+
+Output: one JSON line on rank 0 (see the keys below).  `--impl reference`
+times the reference's own kernels on the host cores (oracle/_ref) on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "efwi-3d_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Gcell-updates/s fwd+adj at 128^3 x 16 shots"
+UNIT = "Gcell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nt", type=int, default=2000)
+    ap.add_argument("--shots", type=int, default=16)
+    ap.add_argument("--n", type=int, default=128, help="model cells per axis")
+    ap.add_argument("--profile-sample", type=int, default=8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-nt", type=int, default=24, help="time steps of the CPU samples")
+    ap.add_argument("--tile-bx", type=int, default=4)
+    ap.add_argument("--zchunk", type=int, default=16)
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def kernel_bytes(grid, nshot_launch=1):
+    """Algorithmic bytes per launch of each stencil kernel class.
+
+    N cells of the padded grid, S = slab cells summed over the three axes.
+    stress_fwd  : 17 floats per cell (read v x3, lambda, mu; r/w 6 stresses)
+                  + 24 B per slab cell (3 memory variables r/w)
+    velocity_fwd: 13 floats per cell (read 6 stresses, B; r/w 3 velocities)
+                  + 24 B per slab cell
+    rev_velocity: 29 floats per cell (reverse velocity: 6 stresses, r/w 3
+                  velocities, r/w rho image; adjoint velocity: 6 adjoint
+                  stresses, lambda, mu, B, r/w 3 adjoint velocities)
+                  + 36 B per slab cell (3 psi read, 3 psi r/w)
+    rev_stress  : 37 floats per cell (reverse stress: 3 velocities, r/w 6
+                  stresses, r/w lambda and mu images; adjoint stress: 3
+                  adjoint velocities, lambda, mu, B, r/w 6 adjoint stresses)
+                  + 36 B per slab cell
+    """
+    n = grid.ncell
+    S = 2 * grid.npml * (grid.nx * grid.ny + grid.nz * grid.ny + grid.nz * grid.nx)
+    per = {"stress_fwd": 68 * n + 24 * S, "velocity_fwd": 52 * n + 24 * S,
+           "rev_velocity": 116 * n + 36 * S, "rev_stress": 148 * n + 36 * S}
+    return {k: v * nshot_launch for k, v in per.items()}
+
+
+def algorithmic_step_bytes(grid, nmodel):
+    """B_g = 3 B_f + 24 N_int per time step, B_f = 120 N + 48 S."""
+    n = grid.ncell
+    S = 2 * grid.npml * (grid.nx * grid.ny + grid.nz * grid.ny + grid.nz * grid.nx)
+    return 3 * (120 * n + 48 * S) + 24 * nmodel
+
+
+class CpuSample:
+    """The CPU gradient (FP64 port or the reference's kernels) on one shot of
+    the benchmark grid with a short time axis; inputs are built once."""
+
+    def __init__(self, kind, n, nt, threads=0):
+        import numpy as np
+        import oracle
+        from efwi import synthetic
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from helpers import case_of
+        self.kind, self.nt = kind, nt
+        self.p = synthetic.config2(nt=nt, nshot=1, n=n)
+        self.lib = oracle.port() if kind == "port" else oracle.ref()
+        if threads:
+            self.lib.set_threads(threads)
+        dt = np.float64 if kind == "port" else np.float32
+        self.obs = self.lib.forward(case_of(self.p, "true", dt))
+        self.case = case_of(self.p, "init", dt)
+
+    def run(self):
+        t0 = time.perf_counter()
+        if self.kind == "port":
+            self.lib.gradient(self.case, self.obs, mode=0)
+        else:
+            self.lib.gradient(self.case, self.obs)
+        el = time.perf_counter() - t0
+        return self.p.grid.ncell * self.nt / el / 1e9, el
+
+    @property
+    def cores(self):
+        return self.lib.num_threads()
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref (reference kernels built for the host) is missing"}))
+        return
+    cs = CpuSample("ref", a.n, a.cpu_nt)
+    for _ in range(a.warmup):
+        cs.run()
+    rates, els = [], []
+    for _ in range(a.steps):
+        r, el = cs.run()
+        rates.append(r)
+        els.append(el)
+    v = sum(rates) / len(rates)
+    p, cores = cs.p, cs.cores
+    sample = f"1 shot of the {p.grid.nz}^3 padded grid, nt={a.cpu_nt}, reference gradient (calc_id 1)"
+    line = dict(base)
+    line.update({"value": v, "ms_per_step": 1e3 * sum(els) / len(els),
+                 "config": {"workload": "config2 sample: " + sample, "model_cells": a.n,
+                            "padded": p.grid.nz, "shots_per_step": 1, "nt": a.cpu_nt},
+                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                                  "sample": sample},
+                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    print(json.dumps(line))
+
+
+def write_dropin_files(tmpdir, prob, obs_split, shot_ids):
+    """Para/survey JSON and Shot_*.bin files for the reference-facing API."""
+    import numpy as np
+    from efwi import config
+    import fwi_utils as ft
+    g = prob.grid
+    para = os.path.join(tmpdir, "para_file.json")
+    survey = os.path.join(tmpdir, "survey_file.json")
+    data = os.path.join(tmpdir, "Data")
+    ft.paraGen_3d(g.nz, g.nx, g.ny, g.dz, g.dx, g.dy, g.nt, g.dt, g.f0, g.npml, para, survey, data)
+    sv = {"nShots": len(prob.shots)}
+    for k, s in enumerate(prob.shots):
+        sv[f"shot{k}"] = {"z_src": int(s.src[0]) - g.npml, "x_src": int(s.src[1]) - g.npml,
+                          "y_src": int(s.src[2]) - g.npml, "nrec": s.nrec,
+                          "z_rec": (np.asarray(s.z_rec) - g.npml).tolist(),
+                          "x_rec": (np.asarray(s.x_rec) - g.npml).tolist(),
+                          "y_rec": (np.asarray(s.y_rec) - g.npml).tolist()}
+    json.dump(sv, open(survey, "w"))
+    for k, t in zip(shot_ids, obs_split):
+        config.write_shot_data(data, k, t.cpu().numpy())
+    return para
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=dev)
+
+    from efwi import synthetic
+    from efwi.engine import Propagator
+
+    # ---------------------------------------------------------------- setup
+    prob = synthetic.config2(nt=a.nt, nshot=a.shots, n=a.n, seed=2 + rank)
+    g = prob.grid
+    ids = list(range(len(prob.shots)))
+    P = Propagator(g, device=dev, tile_bx=a.tile_bx, zchunk=a.zchunk, max_batch=4)
+    P.set_survey(prob.shots, prob.stf)
+    lt, mt, rt = prob.params("true")
+    P.set_model(torch.from_numpy(lt), torch.from_numpy(mt), torch.from_numpy(rt))
+    obs = P.forward(ids)
+    torch.cuda.synchronize()
+    lam, mu, rho = (torch.from_numpy(x).to(dev) for x in prob.params("init"))
+    P.set_model(lam, mu, rho)
+
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        J, gl, gm, gr = P.gradient(ids, obs)
+        if world > 1:
+            jt = torch.tensor([J], device=dev, dtype=torch.float32)
+            for t in (gl, gm, gr, jt):
+                dist.all_reduce(t)
+        return gl
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = Clocks(local)
+    clk.start()
+    P.profile(a.profile_sample)
+    P.profile_read()  # reset counters
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    prof = P.profile_read()
+    P.profile(0)
+    clocks = clk.stop()
+    ms_local = e0.elapsed_time(e1) / a.steps
+    ms = ms_local
+    if world > 1:
+        t = torch.tensor([ms_local], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells_step = prob.cell_steps * world
+    value = cells_step / (ms * 1e-3) / 1e9
+    launches = int(sum(v["launches"] for v in prof.values()))
+
+    # roofline of the dominant kernel (share of timed launches)
+    peak, peak_kind = peaks()
+    kb = kernel_bytes(g)
+    stencil = {k: v for k, v in prof.items() if k in kb and v["timed"] > 0}
+    tot_ms = {k: v["ms"] / v["timed"] * v["launches"] for k, v in stencil.items()}
+    dom = max(tot_ms, key=tot_ms.get) if tot_ms else None
+    roof = None
+    if dom:
+        avg_s = prof[dom]["ms"] / prof[dom]["timed"] * 1e-3
+        ach = kb[dom] / avg_s / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                "peak_kind": peak_kind, "avg_launch_ms": round(avg_s * 1e3, 4),
+                "shares": {k: round(v / sum(tot_ms.values()), 4) for k, v in tot_ms.items()}}
+    nmodel = (g.nz - 2 * g.npml) * (g.nx - 2 * g.npml) * (g.ny - 2 * g.npml)
+    step_bytes = algorithmic_step_bytes(g, nmodel) * g.nt * len(ids)
+    whole = {"bytes_per_step": step_bytes,
+             "achieved_gbs": round(step_bytes / (ms_local * 1e-3) / 1e9, 1),
+             "frac": round(step_bytes / (ms_local * 1e-3) / 1e9 / peak, 4)}
+
+    # --------------------------------------------------- e2e through fwi_ops
+    e2e = None
+    if not a.no_e2e:
+        import FWI_ops_3d as F
+        with tempfile.TemporaryDirectory() as tmp:
+            para = write_dropin_files(tmp, prob, P.split(obs, ids), ids)
+            lam_h, mu_h, rho_h = (torch.from_numpy(x).pin_memory() for x in prob.params("init"))
+            stf_h = torch.from_numpy(np.ascontiguousarray(prob.stf))
+            sid = torch.tensor(ids, dtype=torch.int32)
+            F.fwi_ops.backward(lam_h, mu_h, rho_h, stf_h, 1, sid, para)  # loads obs into HBM
+            torch.cuda.synchronize()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            for _ in range(a.steps):
+                out = F.fwi_ops.backward(lam_h, mu_h, rho_h, stf_h, 1, sid, para)
+                if world > 1:
+                    gsum = torch.stack(out[1:4]).to(dev)
+                    dist.all_reduce(gsum)
+                    _ = gsum.cpu()
+            f1.record(stream)
+            torch.cuda.synchronize()
+            ms_e2e = f0.elapsed_time(f1) / a.steps
+            if world > 1:
+                t = torch.tensor([ms_e2e], device=dev)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms_e2e = float(t.item())
+            nb = g.ncell * 4
+            e2e = {"value": cells_step / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+                   "h2d_bytes_per_step": 3 * nb, "d2h_bytes_per_step": 3 * nb + 4,
+                   "ms_per_step": ms_e2e, "api": "FWI_ops_3d.fwi_ops.backward (host tensors)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cs = CpuSample("port", a.n, a.cpu_nt)
+        r, el = cs.run()
+        cpu = {"value": r, "unit": UNIT, "cores": cs.cores, "kind": "port",
+               "sample": f"FP64 oracle, reference gradient, 1 shot of the {g.nz}^3 padded grid, "
+                         f"nt={a.cpu_nt} ({el:.1f} s)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"config2: {a.n}^3 model ({g.nz}^3 padded, C-PML {g.npml}),"
+                                       f" {len(ids)} shots per GPU, nt={g.nt}, reference gradient",
+                           "model_cells": a.n, "padded": g.nz, "shots_per_gpu": len(ids),
+                           "nt": g.nt, "mode": "reference",
+                           "l2": "inputs larger than L2 (9 fields x 14 MB per shot + shell store)",
+                           "tile_bx": a.tile_bx, "zchunk": a.zchunk},
+                "roofline": roof, "step_roofline": whole, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clocks,
+                "kernel_profile": {k: {"launches": v["launches"],
+                                       "avg_ms": (v["ms"] / v["timed"]) if v["timed"] else None}
+                                   for k, v in prof.items() if v["launches"]}}
+        print(json.dumps(line))
+    P.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,756 @@
+// C ABI of the engine (include/efwi.h): handle, workspace and the time
+// loops of the forward and gradient calls.
+//
+// Structure of a call (compare cufd, Ops/FWI/Src_3d/libCUFD.cu:37-799):
+//   - the model, coefficients and survey stay resident in HBM across calls
+//     (the reference re-creates them, re-allocates 45 volumes and re-reads
+//     the survey on every call, libCUFD.cu:52-205);
+//   - forward-only calls advance up to `max_batch` shots per launch;
+//   - the reference gradient runs shot by shot with the boundary shell
+//     stored in HBM, and accumulates the images in shot order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/efwi.h"
+#include "efwi_kernels.h"
+
+using namespace efwi;
+
+namespace {
+
+enum KClass {
+  K_STRESS_FWD = 0,
+  K_VELOCITY_FWD,
+  K_REV_VELOCITY,
+  K_REV_STRESS,
+  K_RECORD,
+  K_INJECT,
+  K_SHELL_SAVE,
+  K_SHELL_RESTORE,
+  K_MISFIT,
+  K_OTHER,
+  K_NCLASS
+};
+const char *kKernelNames[K_NCLASS] = {"stress_fwd", "velocity_fwd", "rev_velocity", "rev_stress",
+                                      "record", "inject", "shell_save", "shell_restore",
+                                      "misfit", "other"};
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+struct ShotHost {
+  long long src_cell = -1;
+  int nrec = 0;
+  std::vector<long long> rec_cell;
+  std::vector<float> win0, win1, wts;
+  float src_w = 1.0f;
+};
+
+struct Pending {
+  int cls;
+  cudaEvent_t a, b;
+};
+
+}  // namespace
+
+struct EfwiHandle {
+  EfwiGrid grid{};
+  Geo geo{};
+  long long N = 0;
+  int if_win = 0, bx = 4, zchunk = 16, max_batch = 4;
+  std::string err;
+
+  DevBuf coef, lam, mu, buoy;
+  bool model_set = false;
+
+  std::vector<ShotHost> shots;
+  DevBuf stf, src_cell;
+  bool survey_set = false;
+
+  DevBuf pts;
+  int npts = 0;
+
+  DevBuf fields, psi, adj, traces_tm, res_tm, shell, partial, jdev, recbuf, winbuf, scalar;
+
+  int prof_sample = 0;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<Pending> pending;
+  long long launches[K_NCLASS] = {0};
+  long long timed[K_NCLASS] = {0};
+  double ms[K_NCLASS] = {0};
+};
+
+namespace {
+
+int fail(EfwiHandle *h, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (h) h->err = buf;
+  return code;
+}
+
+#define CK_CUDA(h, call)                                                              \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? EFWI_ERR_NOMEM : EFWI_ERR_CUDA, \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+// Reference C-PML profile (utilities.cu:204-320), evaluated with the
+// reference's float variables and double intermediates.
+void cpml_profile(int n, int npml, float dh, float f0, float dt, float *out6) {
+  float *K = out6, *a = out6 + n, *b = out6 + 2 * n, *Kh = out6 + 3 * n, *ah = out6 + 4 * n,
+        *bh = out6 + 5 * n;
+  const double kPi = 3.141592653589793238462643383279502884197169;
+  const float Rc = 0.0008f, Kmax = 2.0f, npow = 8.0f, vp = 3000.0f;
+  const float amax = (float)(2.0 * kPi * (f0 / 2.0));
+  const float L = npml * dh;
+  const float d0 = (float)(-(npow + 1) * vp * std::log((double)Rc) / (2.0 * L));
+  std::vector<float> d(n, 0.f), dhh(n, 0.f), al(n, 0.f), alh(n, 0.f);
+  for (int i = 0; i < n; ++i) { K[i] = 1.f; Kh[i] = 1.f; a[i] = 0.f; ah[i] = 0.f; b[i] = 0.f; bh[i] = 0.f; }
+  auto prof = [&](float depth, float &dd, float &KK, float &aa) {
+    const float x = depth / L;
+    dd = d0 * (float)(0.25 * x + 0.75 * std::pow((double)x, (double)npow));
+    KK = (float)(1.0 + (Kmax - 1.0) * std::pow((double)x, (double)npow));
+    aa = (float)(amax * (1.0 - x));
+  };
+  for (int i = 0; i < n; ++i) {
+    float depth = (npml - i) * dh;
+    if (depth >= 0.f) prof(depth, d[i], K[i], al[i]);
+    depth = (float)((npml - i - 0.5) * dh);
+    if (depth >= 0.f) prof(depth, dhh[i], Kh[i], alh[i]);
+    depth = (npml - n + i) * dh;
+    if (depth >= 0.f) prof(depth, d[i], K[i], al[i]);
+    depth = (float)((npml - n + i + 0.5) * dh);
+    if (depth >= 0.f) prof(depth, dhh[i], Kh[i], alh[i]);
+    if (al[i] < 0.f) al[i] = 0.f;
+    if (alh[i] < 0.f) alh[i] = 0.f;
+    b[i] = std::exp(-(d[i] / K[i] + al[i]) * dt);
+    bh[i] = std::exp(-(dhh[i] / Kh[i] + alh[i]) * dt);
+    if (std::fabs(d[i]) > 1.0e-6) a[i] = (float)(d[i] * (b[i] - 1.0) / (K[i] * (d[i] + K[i] * al[i])));
+    if (std::fabs(dhh[i]) > 1.0e-6)
+      ah[i] = (float)(dhh[i] * (bh[i] - 1.0) / (Kh[i] * (dhh[i] + Kh[i] * alh[i])));
+  }
+}
+
+// Source taper: cuda_window with nrec = 1 and ratio 0.001 (Src_Rec.cu:146,
+// utilities.cu:578-614).
+void taper_stf(const float *in, int nt, float dt, float *out) {
+  const double kPi = 3.141592653589793238462643383279502884197169;
+  const float ratio = 0.001f;
+  const float t0 = 0.0f, t3 = nt * dt, off = nt * dt * ratio;
+  const bool ok = !(2.0 * off >= t3 - t0);
+  const float t1 = t0 + off, t2 = t3 - off;
+  for (int it = 0; it < nt; ++it) {
+    if (!ok) { out[it] = in[it]; continue; }
+    const float t = it * dt;
+    float w;
+    if (t >= t0 && t < t1) w = (float)std::sin(kPi / 2.0 * (t - t0) / (t1 - t0));
+    else if (t >= t1 && t < t2) w = 1.0f;
+    else if (t >= t2 && t < t3) w = (float)std::cos(kPi / 2.0 * (t - t2) / (t3 - t2));
+    else w = 0.0f;
+    out[it] = in[it] * (w * w);
+  }
+}
+
+// Shell points (Boundary.cu:14-20, utilities.cu:323-420): the box
+// [npml-2, n-npml+1]^3 minus its part more than 4 cells inside every face.
+// Points outside [2, n-3]^3 never change (they stay zero), so they are left
+// out.
+std::vector<int> shell_points(const EfwiGrid &g) {
+  std::vector<int> pts;
+  const int lo = g.npml - 2;
+  const int hz = g.nz - g.npml + 1, hx = g.nx - g.npml + 1, hy = g.ny - g.npml + 1;
+  for (int z = std::max(lo, 2); z <= std::min(hz, g.nz - 3); ++z)
+    for (int x = std::max(lo, 2); x <= std::min(hx, g.nx - 3); ++x)
+      for (int y = std::max(lo, 2); y <= std::min(hy, g.ny - 3); ++y) {
+        const bool in = z <= lo + 4 || z >= hz - 4 || x <= lo + 4 || x >= hx - 4 ||
+                        y <= lo + 4 || y >= hy - 4;
+        if (in) pts.push_back((int)(((long long)z * g.nx + x) * g.ny + y));
+      }
+  return pts;
+}
+
+__global__ void k_max_vp(const float *lam, const float *mu, const float *rho, long long n,
+                         unsigned int *out) {
+  float m = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float v = sqrtf((lam[i] + 2.0f * mu[i]) / rho[i]);
+    if (v > m) m = v;
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+cudaEvent_t next_event(EfwiHandle *h) {
+  if (h->ev_used == h->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    h->ev_pool.push_back(e);
+  }
+  return h->ev_pool[h->ev_used++];
+}
+
+// Launch bracket: counts launches and, on sampled steps, records events.
+struct Timer {
+  EfwiHandle *h;
+  int cls;
+  cudaStream_t s;
+  bool on;
+  cudaEvent_t a{}, b{};
+  Timer(EfwiHandle *h_, int cls_, cudaStream_t s_, int it) : h(h_), cls(cls_), s(s_) {
+    h->launches[cls]++;
+    on = h->prof_sample > 0 && (it % h->prof_sample == 0);
+    if (on) { a = next_event(h); b = next_event(h); cudaEventRecord(a, s); }
+  }
+  ~Timer() {
+    if (on) { cudaEventRecord(b, s); h->pending.push_back({cls, a, b}); }
+  }
+};
+
+int check_launch(EfwiHandle *h, const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(h, EFWI_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
+  return EFWI_OK;
+}
+
+Fields fields_at(float *base, long long N, int S) {
+  // volumes of a batch of S shots: 9 arrays of S*N floats
+  Fields f;
+  const long long v = N * S;
+  f.vz = base; f.vx = base + v; f.vy = base + 2 * v;
+  f.szz = base + 3 * v; f.sxx = base + 4 * v; f.syy = base + 5 * v;
+  f.sxz = base + 6 * v; f.sxy = base + 7 * v; f.syz = base + 8 * v;
+  return f;
+}
+
+long long psi_per_shot(const Geo &g) { return 6 * (g.slab_z + g.slab_x + g.slab_y); }
+
+Psi psi_at(float *base, const Geo &g, int S) {
+  Psi p;
+  p.z = base;
+  p.x = base + (long long)S * 6 * g.slab_z;
+  p.y = p.x + (long long)S * 6 * g.slab_x;
+  return p;
+}
+
+// Receivers of a batch, grouped by (shot, cell).
+struct RecHost {
+  std::vector<long long> ucell, trace_off;
+  std::vector<int> ushot, uptr, rec, nrec;
+};
+
+RecHost group_receivers(const EfwiHandle *h, const int *ids, int S, long long *total_floats) {
+  RecHost r;
+  long long off = 0;
+  for (int s = 0; s < S; ++s) {
+    const ShotHost &sh = h->shots[ids[s]];
+    r.trace_off.push_back(off);
+    r.nrec.push_back(sh.nrec);
+    off += 3LL * sh.nrec * h->grid.nt;
+    std::vector<std::pair<long long, int>> cr;
+    for (int k = 0; k < sh.nrec; ++k) cr.push_back({sh.rec_cell[k], k});
+    std::sort(cr.begin(), cr.end());
+    for (size_t k = 0; k < cr.size(); ++k) {
+      if (k == 0 || cr[k].first != cr[k - 1].first) {
+        r.ucell.push_back(cr[k].first);
+        r.ushot.push_back(s);
+        r.uptr.push_back((int)r.rec.size());
+      }
+      r.rec.push_back(cr[k].second);
+    }
+  }
+  r.uptr.push_back((int)r.rec.size());
+  *total_floats = off;
+  return r;
+}
+
+// Uploads the grouping into h->recbuf and returns device views.
+int upload_receivers(EfwiHandle *h, const RecHost &r, cudaStream_t st, RecArgs *out) {
+  auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t b0 = al(r.ucell.size() * 8), b1 = al(r.trace_off.size() * 8),
+               b2 = al(r.ushot.size() * 4), b3 = al(r.uptr.size() * 4), b4 = al(r.rec.size() * 4 + 4),
+               b5 = al(r.nrec.size() * 4);
+  CK_CUDA(h, h->recbuf.ensure(b0 + b1 + b2 + b3 + b4 + b5));
+  char *p = h->recbuf.as<char>();
+  CK_CUDA(h, cudaMemcpyAsync(p, r.ucell.data(), r.ucell.size() * 8, cudaMemcpyHostToDevice, st));
+  CK_CUDA(h, cudaMemcpyAsync(p + b0, r.trace_off.data(), r.trace_off.size() * 8, cudaMemcpyHostToDevice, st));
+  CK_CUDA(h, cudaMemcpyAsync(p + b0 + b1, r.ushot.data(), r.ushot.size() * 4, cudaMemcpyHostToDevice, st));
+  CK_CUDA(h, cudaMemcpyAsync(p + b0 + b1 + b2, r.uptr.data(), r.uptr.size() * 4, cudaMemcpyHostToDevice, st));
+  if (!r.rec.empty())
+    CK_CUDA(h, cudaMemcpyAsync(p + b0 + b1 + b2 + b3, r.rec.data(), r.rec.size() * 4, cudaMemcpyHostToDevice, st));
+  CK_CUDA(h, cudaMemcpyAsync(p + b0 + b1 + b2 + b3 + b4, r.nrec.data(), r.nrec.size() * 4, cudaMemcpyHostToDevice, st));
+  out->ucell = (const long long *)p;
+  out->trace_off = (const long long *)(p + b0);
+  out->ushot = (const int *)(p + b0 + b1);
+  out->uptr = (const int *)(p + b0 + b1 + b2);
+  out->rec = (const int *)(p + b0 + b1 + b2 + b3);
+  out->nrec = (const int *)(p + b0 + b1 + b2 + b3 + b4);
+  out->ncell = (int)r.ucell.size();
+  return EFWI_OK;
+}
+
+int check_ready(EfwiHandle *h, int n, const int *ids) {
+  if (!h) return EFWI_ERR_ARG;
+  if (!h->model_set) return fail(h, EFWI_ERR_STATE, "efwi_set_model has not been called");
+  if (!h->survey_set) return fail(h, EFWI_ERR_STATE, "efwi_set_survey has not been called");
+  if (n < 0 || (n > 0 && !ids)) return fail(h, EFWI_ERR_ARG, "invalid shot list");
+  for (int k = 0; k < n; ++k)
+    if (ids[k] < 0 || ids[k] >= (int)h->shots.size())
+      return fail(h, EFWI_ERR_ARG, "shot id %d out of range [0, %d)", ids[k], (int)h->shots.size());
+  return EFWI_OK;
+}
+
+dim3 stencil_grid(const EfwiHandle *h, int S, int *nzc) {
+  *nzc = (h->grid.nz + h->zchunk - 1) / h->zchunk;
+  return dim3((h->grid.ny + 31) / 32, (h->grid.nx + h->bx - 1) / h->bx, (unsigned)(S * *nzc));
+}
+
+// One forward time step of a batch: stress (+ source), velocity, receivers.
+int forward_step(EfwiHandle *h, Fields f, Psi ps, int S, const SrcArgs &src, const RecArgs &rec,
+                 float *traces_tm, cudaStream_t st, int it) {
+  int nzc;
+  const dim3 grid = stencil_grid(h, S, &nzc);
+  {
+    Timer t(h, K_STRESS_FWD, st, it);
+    launch_stress_fwd(h->bx, grid, st, h->geo, f, ps, h->lam.as<float>(), h->mu.as<float>(),
+                      h->zchunk, nzc, src);
+  }
+  {
+    Timer t(h, K_VELOCITY_FWD, st, it);
+    launch_velocity_fwd(h->bx, grid, st, h->geo, f, ps, h->buoy.as<float>(), h->zchunk, nzc);
+  }
+  if (rec.ncell > 0) {
+    Timer t(h, K_RECORD, st, it);
+    k_record<<<(rec.ncell + 127) / 128, 128, 0, st>>>(f, h->N, rec, traces_tm, it + 1);
+  }
+  return check_launch(h, "forward step");
+}
+
+// Forward of a batch of S shots (ids) into traces_tm (time-major, zeroed
+// here).  When `shell` is set (S must be 1) the boundary shell is stored
+// before every step.
+int run_forward_batch(EfwiHandle *h, const int *ids, int S, float *traces_tm, long long ntr,
+                      RecArgs *rec_out, float *shell, cudaStream_t st) {
+  const long long N = h->N;
+  CK_CUDA(h, h->fields.ensure(sizeof(float) * 9 * N * S));
+  CK_CUDA(h, h->psi.ensure(sizeof(float) * psi_per_shot(h->geo) * S));
+  CK_CUDA(h, cudaMemsetAsync(h->fields.p, 0, sizeof(float) * 9 * N * S, st));
+  CK_CUDA(h, cudaMemsetAsync(h->psi.p, 0, sizeof(float) * psi_per_shot(h->geo) * S, st));
+  CK_CUDA(h, cudaMemsetAsync(traces_tm, 0, sizeof(float) * ntr, st));
+  Fields f = fields_at(h->fields.as<float>(), N, S);
+  Psi ps = psi_at(h->psi.as<float>(), h->geo, S);
+
+  long long tot;
+  RecHost rh = group_receivers(h, ids, S, &tot);
+  RecArgs rec;
+  int rc = upload_receivers(h, rh, st, &rec);
+  if (rc) return rc;
+  if (rec_out) *rec_out = rec;
+
+  // per-batch source arrays: cells and tapered stf rows, staged in scalar buf
+  const int nt = h->grid.nt;
+  CK_CUDA(h, h->scalar.ensure(sizeof(long long) * S + sizeof(float) * (size_t)S * nt + 256));
+  std::vector<long long> cells(S);
+  for (int s = 0; s < S; ++s) cells[s] = h->shots[ids[s]].src_cell;
+  long long *dcell = h->scalar.as<long long>();
+  float *dstf = (float *)((char *)h->scalar.p + ((sizeof(long long) * S + 255) & ~size_t(255)));
+  CK_CUDA(h, cudaMemcpyAsync(dcell, cells.data(), sizeof(long long) * S, cudaMemcpyHostToDevice, st));
+  for (int s = 0; s < S; ++s)
+    CK_CUDA(h, cudaMemcpyAsync(dstf + (size_t)s * nt, h->stf.as<float>() + (size_t)ids[s] * nt,
+                               sizeof(float) * nt, cudaMemcpyDeviceToDevice, st));
+  SrcArgs src{dcell, dstf, nt, 0};
+  const int npts = h->npts;
+  for (int it = 0; it <= nt - 2; ++it) {
+    if (shell) {
+      Timer t(h, K_SHELL_SAVE, st, it);
+      k_shell_save<<<(npts + 255) / 256, 256, 0, st>>>(f, h->pts.as<int>(), npts,
+                                                       shell + (size_t)it * 9 * npts);
+    }
+    src.it = it;
+    rc = forward_step(h, f, ps, S, src, rec, traces_tm, st, it);
+    if (rc) return rc;
+  }
+  return check_launch(h, "forward");
+}
+
+int resolve_profile(EfwiHandle *h) {
+  for (const Pending &p : h->pending) {
+    float t = 0.f;
+    cudaError_t e = cudaEventSynchronize(p.b);
+    if (e != cudaSuccess) return fail(h, EFWI_ERR_CUDA, "profile event: %s", cudaGetErrorString(e));
+    cudaEventElapsedTime(&t, p.a, p.b);
+    h->ms[p.cls] += t;
+    h->timed[p.cls]++;
+  }
+  h->pending.clear();
+  h->ev_used = 0;
+  return EFWI_OK;
+}
+
+// Misfit of one shot: fills res_tm and adds the sum of squares to *jdev.
+int misfit_shot(EfwiHandle *h, const ShotHost &sh, const float *obs, const float *syn_tm,
+                float *res_tm, double *jdev, cudaStream_t st) {
+  const int nt = h->grid.nt, nr = sh.nrec;
+  if (nr == 0) return EFWI_OK;
+  dim3 grid((nt + 31) / 32, (nr + 31) / 32, 3);
+  const int nb = grid.x * grid.y * grid.z;
+  CK_CUDA(h, h->partial.ensure(sizeof(double) * nb));
+  MisfitArgs m{};
+  m.nt = nt; m.nrec = nr; m.dt = h->grid.dt; m.if_win = h->if_win; m.src_weight = sh.src_w;
+  if (h->if_win) {
+    CK_CUDA(h, h->winbuf.ensure(sizeof(float) * 3 * nr));
+    float *w = h->winbuf.as<float>();
+    CK_CUDA(h, cudaMemcpyAsync(w, sh.win0.data(), sizeof(float) * nr, cudaMemcpyHostToDevice, st));
+    CK_CUDA(h, cudaMemcpyAsync(w + nr, sh.win1.data(), sizeof(float) * nr, cudaMemcpyHostToDevice, st));
+    CK_CUDA(h, cudaMemcpyAsync(w + 2 * nr, sh.wts.data(), sizeof(float) * nr, cudaMemcpyHostToDevice, st));
+    m.win_start = w; m.win_end = w + nr; m.weights = w + 2 * nr;
+  }
+  {
+    Timer t(h, K_MISFIT, st, 0);
+    k_misfit<<<grid, dim3(32, 8), 0, st>>>(m, obs, syn_tm, res_tm, h->partial.as<double>());
+    k_reduce_sum<<<1, 256, 0, st>>>(h->partial.as<double>(), nb, jdev);
+  }
+  return check_launch(h, "misfit");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *efwi_version(void) { return "efwi-b200 0.1 (sm_100a)"; }
+
+int efwi_kernel_count(void) { return K_NCLASS; }
+
+const char *efwi_kernel_name(int k) { return (k >= 0 && k < K_NCLASS) ? kKernelNames[k] : ""; }
+
+const char *efwi_last_error(const EfwiHandle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int efwi_create(const EfwiGrid *g, EfwiHandle **out) {
+  if (!g || !out) return EFWI_ERR_ARG;
+  *out = nullptr;
+  EfwiHandle *h = new EfwiHandle();
+  if (g->nz < 5 || g->nx < 5 || g->ny < 5 || g->nt < 2 || g->npml < 2 || 2 * g->npml > g->nz ||
+      2 * g->npml > g->nx || 2 * g->npml > g->ny || !(g->dt > 0) || !(g->dz > 0) ||
+      !(g->dx > 0) || !(g->dy > 0)) {
+    int rc = fail(h, EFWI_ERR_ARG, "invalid grid nz=%d nx=%d ny=%d npml=%d nt=%d", g->nz, g->nx,
+                  g->ny, g->npml, g->nt);
+    *out = h;
+    return rc;
+  }
+  h->grid = *g;
+  h->N = (long long)g->nz * g->nx * g->ny;
+  if (h->N >= (1LL << 31)) {
+    *out = h;
+    return fail(h, EFWI_ERR_ARG, "grid of %lld cells exceeds 2^31", h->N);
+  }
+  Geo &G = h->geo;
+  G.nz = g->nz; G.nx = g->nx; G.ny = g->ny; G.np = g->npml;
+  G.N = h->N; G.sz = (long long)g->nx * g->ny; G.sx = g->ny;
+  G.dt = g->dt; G.idz = 1.0f / g->dz; G.idx = 1.0f / g->dx; G.idy = 1.0f / g->dy;
+  G.slab_z = 2LL * g->npml * g->nx * g->ny;
+  G.slab_x = (long long)g->nz * 2 * g->npml * g->ny;
+  G.slab_y = (long long)g->nz * g->nx * 2 * g->npml;
+  *out = h;
+  const int nmax = g->nz + g->nx + g->ny;
+  std::vector<float> c(6 * nmax);
+  cpml_profile(g->nz, g->npml, g->dz, g->f0, g->dt, c.data());
+  cpml_profile(g->nx, g->npml, g->dx, g->f0, g->dt, c.data() + 6 * g->nz);
+  cpml_profile(g->ny, g->npml, g->dy, g->f0, g->dt, c.data() + 6 * (g->nz + g->nx));
+  CK_CUDA(h, h->coef.ensure(sizeof(float) * c.size()));
+  CK_CUDA(h, cudaMemcpy(h->coef.p, c.data(), sizeof(float) * c.size(), cudaMemcpyHostToDevice));
+  G.cz = h->coef.as<float>();
+  G.cx = G.cz + 6 * g->nz;
+  G.cy = G.cx + 6 * g->nx;
+  std::vector<int> pts = shell_points(*g);
+  h->npts = (int)pts.size();
+  if (!pts.empty()) {
+    CK_CUDA(h, h->pts.ensure(sizeof(int) * pts.size()));
+    CK_CUDA(h, cudaMemcpy(h->pts.p, pts.data(), sizeof(int) * pts.size(), cudaMemcpyHostToDevice));
+  }
+  return EFWI_OK;
+}
+
+void efwi_destroy(EfwiHandle *h) {
+  if (!h) return;
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  delete h;
+}
+
+int efwi_set_options(EfwiHandle *h, int if_win, int tile_bx, int zchunk, int max_batch) {
+  if (!h) return EFWI_ERR_ARG;
+  if (tile_bx != 0 && tile_bx != 4 && tile_bx != 8) return fail(h, EFWI_ERR_ARG, "tile_bx must be 4 or 8");
+  if (zchunk < 0 || max_batch < 0) return fail(h, EFWI_ERR_ARG, "negative zchunk/max_batch");
+  h->if_win = if_win ? 1 : 0;
+  if (tile_bx) h->bx = tile_bx;
+  if (zchunk) h->zchunk = zchunk;
+  if (max_batch) h->max_batch = max_batch;
+  return EFWI_OK;
+}
+
+int efwi_set_model(EfwiHandle *h, const float *lam, const float *mu, const float *rho, void *stream) {
+  if (!h) return EFWI_ERR_ARG;
+  if (!lam || !mu || !rho) return fail(h, EFWI_ERR_ARG, "null model pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t bytes = sizeof(float) * h->N;
+  CK_CUDA(h, h->lam.ensure(bytes));
+  CK_CUDA(h, h->mu.ensure(bytes));
+  CK_CUDA(h, h->buoy.ensure(bytes));
+  CK_CUDA(h, cudaMemcpyAsync(h->lam.p, lam, bytes, cudaMemcpyDeviceToDevice, st));
+  CK_CUDA(h, cudaMemcpyAsync(h->mu.p, mu, bytes, cudaMemcpyDeviceToDevice, st));
+  k_prep_buoyancy<<<1184, 256, 0, st>>>(rho, h->buoy.as<float>(), h->grid.nz, h->grid.nx, h->grid.ny);
+  h->launches[K_OTHER]++;
+  // CFL check of the reference (2D formula with min(dz, dx)).
+  CK_CUDA(h, h->jdev.ensure(64));
+  unsigned int *vmax = (unsigned int *)h->jdev.p;
+  CK_CUDA(h, cudaMemsetAsync(vmax, 0, sizeof(unsigned int), st));
+  k_max_vp<<<592, 256, 0, st>>>(lam, mu, rho, h->N, vmax);
+  h->launches[K_OTHER]++;
+  int rc = check_launch(h, "set_model");
+  if (rc) return rc;
+  unsigned int bits = 0;
+  CK_CUDA(h, cudaMemcpyAsync(&bits, vmax, sizeof(bits), cudaMemcpyDeviceToHost, st));
+  CK_CUDA(h, cudaStreamSynchronize(st));
+  float vm;
+  std::memcpy(&vm, &bits, sizeof(vm));
+  const float dh = h->grid.dz < h->grid.dx ? h->grid.dz : h->grid.dx;
+  const float courant = vm * h->grid.dt * sqrtf(2.0f) * (1.0f / 24.0f + 9.0f / 8.0f) / dh;
+  h->model_set = false;
+  if (!(courant <= 1.0f)) return fail(h, EFWI_ERR_CFL, "Courant_number = %g", courant);
+  h->model_set = true;
+  return EFWI_OK;
+}
+
+int efwi_set_survey(EfwiHandle *h, int nshot, const EfwiShot *shots, const float *stf) {
+  if (!h) return EFWI_ERR_ARG;
+  if (nshot < 0 || (nshot > 0 && (!shots || !stf))) return fail(h, EFWI_ERR_ARG, "invalid survey");
+  const EfwiGrid &g = h->grid;
+  std::vector<ShotHost> out(nshot);
+  for (int k = 0; k < nshot; ++k) {
+    const EfwiShot &s = shots[k];
+    if (s.z_src < 2 || s.z_src > g.nz - 3 || s.x_src < 2 || s.x_src > g.nx - 3 || s.y_src < 2 ||
+        s.y_src > g.ny - 3)
+      return fail(h, EFWI_ERR_ARG, "shot %d: source (%d, %d, %d) outside the updated region", k,
+                  s.z_src, s.x_src, s.y_src);
+    if (s.nrec < 0 || (s.nrec > 0 && (!s.z_rec || !s.x_rec || !s.y_rec)))
+      return fail(h, EFWI_ERR_ARG, "shot %d: invalid receivers", k);
+    ShotHost &o = out[k];
+    o.src_cell = ((long long)s.z_src * g.nx + s.x_src) * g.ny + s.y_src;
+    o.nrec = s.nrec;
+    o.rec_cell.resize(s.nrec);
+    for (int r = 0; r < s.nrec; ++r) {
+      const int z = s.z_rec[r], x = s.x_rec[r], y = s.y_rec[r];
+      if (z < 0 || z >= g.nz || x < 0 || x >= g.nx || y < 0 || y >= g.ny)
+        return fail(h, EFWI_ERR_ARG, "shot %d receiver %d at (%d, %d, %d) outside the grid", k, r, z, x, y);
+      o.rec_cell[r] = ((long long)z * g.nx + x) * g.ny + y;
+    }
+    o.win0.assign(s.nrec, 0.f);
+    o.win1.assign(s.nrec, 0.f);
+    o.wts.assign(s.nrec, 1.f);
+    for (int r = 0; r < s.nrec; ++r) {
+      if (s.win_start) o.win0[r] = s.win_start[r];
+      if (s.win_end) o.win1[r] = s.win_end[r];
+      if (s.weights) o.wts[r] = s.weights[r];
+    }
+    o.src_w = s.src_weight;
+  }
+  std::vector<float> tap((size_t)nshot * g.nt);
+  for (int k = 0; k < nshot; ++k) taper_stf(stf + (size_t)k * g.nt, g.nt, g.dt, tap.data() + (size_t)k * g.nt);
+  if (nshot > 0) {
+    CK_CUDA(h, h->stf.ensure(sizeof(float) * tap.size()));
+    CK_CUDA(h, cudaMemcpy(h->stf.p, tap.data(), sizeof(float) * tap.size(), cudaMemcpyHostToDevice));
+  }
+  h->shots.swap(out);
+  h->survey_set = true;
+  return EFWI_OK;
+}
+
+int efwi_forward(EfwiHandle *h, int n, const int *ids, float *traces, void *stream) {
+  int rc = check_ready(h, n, ids);
+  if (rc) return rc;
+  if (n > 0 && !traces) return fail(h, EFWI_ERR_ARG, "null traces");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nt = h->grid.nt;
+  long long out_off = 0;
+  for (int b0 = 0; b0 < n; b0 += h->max_batch) {
+    const int S = std::min(h->max_batch, n - b0);
+    long long ntr = 0;
+    for (int s = 0; s < S; ++s) ntr += 3LL * h->shots[ids[b0 + s]].nrec * nt;
+    CK_CUDA(h, h->traces_tm.ensure(sizeof(float) * std::max(ntr, 1LL)));
+    rc = run_forward_batch(h, ids + b0, S, h->traces_tm.as<float>(), ntr, nullptr, nullptr, st);
+    if (rc) return rc;
+    long long toff = 0;
+    for (int s = 0; s < S; ++s) {
+      const int nr = h->shots[ids[b0 + s]].nrec;
+      if (nr > 0) {
+        Timer t(h, K_OTHER, st, 0);
+        k_traces_to_cr_t<<<dim3((nt + 31) / 32, (nr + 31) / 32, 3), dim3(32, 8), 0, st>>>(
+            h->traces_tm.as<float>() + toff, traces + out_off, nt, nr);
+      }
+      toff += 3LL * nr * nt;
+      out_off += 3LL * nr * nt;
+    }
+    rc = check_launch(h, "traces");
+    if (rc) return rc;
+  }
+  return EFWI_OK;
+}
+
+static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs, int mode,
+                         double *misfit, float *glam, float *gmu, float *grho, float *res_out,
+                         cudaStream_t st) {
+  const int nt = h->grid.nt;
+  const long long N = h->N;
+  const bool grad = glam != nullptr;
+  if (grad) {
+    CK_CUDA(h, cudaMemsetAsync(glam, 0, sizeof(float) * N, st));
+    CK_CUDA(h, cudaMemsetAsync(gmu, 0, sizeof(float) * N, st));
+    CK_CUDA(h, cudaMemsetAsync(grho, 0, sizeof(float) * N, st));
+  }
+  CK_CUDA(h, h->jdev.ensure(sizeof(double) * (n + 8)));
+  double *jdev = h->jdev.as<double>() + 1;
+  if (n > 0) CK_CUDA(h, cudaMemsetAsync(jdev, 0, sizeof(double) * n, st));
+  if (grad) {
+    CK_CUDA(h, h->adj.ensure(sizeof(float) * 9 * N));
+    CK_CUDA(h, h->shell.ensure(sizeof(float) * 9 * (size_t)std::max(h->npts, 1) * nt));
+  }
+  long long obs_off = 0;
+  for (int k = 0; k < n; ++k) {
+    const ShotHost &sh = h->shots[ids[k]];
+    const long long ntr = 3LL * sh.nrec * nt;
+    CK_CUDA(h, h->traces_tm.ensure(sizeof(float) * std::max(ntr, 1LL)));
+    CK_CUDA(h, h->res_tm.ensure(sizeof(float) * std::max(ntr, 1LL)));
+    RecArgs rec;
+    int rc = run_forward_batch(h, ids + k, 1, h->traces_tm.as<float>(), ntr, &rec,
+                               grad ? h->shell.as<float>() : nullptr, st);
+    if (rc) return rc;
+    rc = misfit_shot(h, sh, obs + obs_off, h->traces_tm.as<float>(), h->res_tm.as<float>(), jdev + k, st);
+    if (rc) return rc;
+    if (res_out && sh.nrec > 0) {
+      k_traces_to_cr_t<<<dim3((nt + 31) / 32, (sh.nrec + 31) / 32, 3), dim3(32, 8), 0, st>>>(
+          h->res_tm.as<float>(), res_out + obs_off, nt, sh.nrec);
+      h->launches[K_OTHER]++;
+    }
+    obs_off += ntr;
+    if (!grad) continue;
+    // ---------------------------------------------------------- reverse
+    Fields f = fields_at(h->fields.as<float>(), N, 1);
+    Fields a = fields_at(h->adj.as<float>(), N, 1);
+    Psi ps = psi_at(h->psi.as<float>(), h->geo, 1);
+    CK_CUDA(h, cudaMemsetAsync(h->adj.p, 0, sizeof(float) * 9 * N, st));
+    CK_CUDA(h, cudaMemsetAsync(h->psi.p, 0, sizeof(float) * psi_per_shot(h->geo), st));
+    long long *dcell = h->scalar.as<long long>();
+    float *dstf = (float *)((char *)h->scalar.p + 256);
+    SrcArgs src{dcell, dstf, nt, 0};
+    int nzc;
+    const dim3 grid = stencil_grid(h, 1, &nzc);
+    const int npts = h->npts;
+    const float *shell = h->shell.as<float>();
+    auto K1 = [&](int rev, int adj, int it) {
+      Timer t(h, K_REV_VELOCITY, st, it);
+      launch_rev_velocity(h->bx, grid, st, h->geo, f, a, ps, h->lam.as<float>(),
+                          h->mu.as<float>(), h->buoy.as<float>(), grho, h->zchunk, nzc, rev, adj);
+    };
+    auto K2 = [&](int rev, int adj, int it) {
+      Timer t(h, K_REV_STRESS, st, it);
+      src.it = it;
+      launch_rev_stress(h->bx, grid, st, h->geo, f, a, ps, h->lam.as<float>(), h->mu.as<float>(),
+                        h->buoy.as<float>(), glam, gmu, h->zchunk, nzc, rev, adj, src);
+    };
+    auto inject = [&](int it) {
+      if (rec.ncell == 0) return;
+      Timer t(h, K_INJECT, st, it);
+      k_inject<<<(rec.ncell + 127) / 128, 128, 0, st>>>(a, N, rec, h->res_tm.as<float>(), it);
+    };
+    auto restore = [&](int it, int stress) {
+      if (npts == 0) return;
+      Timer t(h, K_SHELL_RESTORE, st, it);
+      k_shell_restore<<<(npts + 255) / 256, 256, 0, st>>>(f, h->pts.as<int>(), npts, shell + (size_t)it * 9 * npts, stress);
+    };
+    K1(0, 1, nt - 1);
+    inject(nt - 1);
+    K2(0, 1, nt - 1);
+    for (int it = nt - 2; it >= 0; --it) {
+      const int adj = it > 0;  // the adjoint update of step 0 feeds no image
+      K1(1, adj, it);
+      if (adj) inject(it);
+      restore(it, 0);
+      K2(1, adj, it);
+      restore(it, 1);
+    }
+    rc = check_launch(h, "reverse");
+    if (rc) return rc;
+  }
+  std::vector<double> js(std::max(n, 1), 0.0);
+  if (n > 0) CK_CUDA(h, cudaMemcpyAsync(js.data(), jdev, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK_CUDA(h, cudaStreamSynchronize(st));
+  double J = 0.0;
+  for (int k = 0; k < n; ++k) J += js[k];
+  if (misfit) *misfit = J;
+  if (h->prof_sample > 0) return resolve_profile(h);
+  return EFWI_OK;
+}
+
+int efwi_misfit(EfwiHandle *h, int n, const int *ids, const float *obs, double *misfit, void *stream) {
+  int rc = check_ready(h, n, ids);
+  if (rc) return rc;
+  if (n > 0 && !obs) return fail(h, EFWI_ERR_ARG, "null obs");
+  return gradient_impl(h, n, ids, obs, EFWI_MODE_REFERENCE, misfit, nullptr, nullptr, nullptr,
+                       nullptr, (cudaStream_t)stream);
+}
+
+int efwi_gradient(EfwiHandle *h, int n, const int *ids, const float *obs, int mode, double *misfit,
+                  float *glam, float *gmu, float *grho, float *res, void *stream) {
+  int rc = check_ready(h, n, ids);
+  if (rc) return rc;
+  if (n > 0 && !obs) return fail(h, EFWI_ERR_ARG, "null obs");
+  if (!glam || !gmu || !grho) return fail(h, EFWI_ERR_ARG, "null gradient output");
+  if (mode != EFWI_MODE_REFERENCE) return fail(h, EFWI_ERR_ARG, "gradient mode %d is not available", mode);
+  return gradient_impl(h, n, ids, obs, mode, misfit, glam, gmu, grho, res, (cudaStream_t)stream);
+}
+
+int efwi_profile(EfwiHandle *h, int sample) {
+  if (!h || sample < 0) return EFWI_ERR_ARG;
+  h->prof_sample = sample;
+  return EFWI_OK;
+}
+
+int efwi_profile_read(EfwiHandle *h, int n, long long *timed, double *ms, long long *launches) {
+  if (!h) return EFWI_ERR_ARG;
+  int rc = resolve_profile(h);
+  if (rc) return rc;
+  for (int k = 0; k < n && k < K_NCLASS; ++k) {
+    if (timed) timed[k] = h->timed[k];
+    if (ms) ms[k] = h->ms[k];
+    if (launches) launches[k] = h->launches[k];
+    h->timed[k] = 0; h->ms[k] = 0; h->launches[k] = 0;
+  }
+  return EFWI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+/*
+ * efwi.h -- C ABI of the B200 elastic wave-propagation engine (EFWI-3D
+ * operator).  Plain pointers and sizes only; no torch types.
+ *
+ * Conventions
+ *   - Volumes are float32 [nz][nx][ny] (y fastest), DEVICE pointers, on the
+ *     padded grid: the caller's torch tensors are passed as they are (the
+ *     reference transposed them on the host, Ops/FWI/Src_3d/libCUFD.cu:72-80).
+ *   - Traces are float32 [3][nrec][nt] per shot (components x, y, z), the
+ *     layout of the reference's Shot_{x,y,z}{id}.bin files
+ *     (libCUFD.cu:709-720); several shots are concatenated in call order.
+ *   - Source and receiver indices are padded-grid indices (the reference
+ *     adds nPoints_pml to survey coordinates, Src_Rec.cu:78-118).
+ *   - Every call returns EFWI_OK or an error code and never exits the
+ *     process (the reference calls exit(1), utilities.h:22-30); the message
+ *     is in efwi_last_error().
+ *   - All device work of a call is enqueued on `stream` (a cudaStream_t, or
+ *     NULL for the legacy default stream).  A handle is used from one host
+ *     thread at a time.
+ */
+#ifndef EFWI_H_
+#define EFWI_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EFWI_OK 0
+#define EFWI_ERR_ARG 1     /* invalid argument or survey */
+#define EFWI_ERR_CUDA 2    /* CUDA runtime error */
+#define EFWI_ERR_CFL 3     /* Courant number > 1 (utilities.cu:186-202) */
+#define EFWI_ERR_STATE 4   /* call order: model or survey missing */
+#define EFWI_ERR_NOMEM 5   /* device allocation failed */
+
+#define EFWI_MODE_REFERENCE 0 /* the reference's gradient (libCUFD.cu:469-613) */
+#define EFWI_MODE_EXACT 1     /* exact discrete adjoint of the forward scheme */
+
+typedef struct EfwiHandle EfwiHandle;
+
+/* Grid and time axis; the fields of the reference's para JSON
+ * (Parameter.cpp:39-104: nz, nx, ny, dz, dx, dy, nSteps, dt, f0,
+ * nPoints_pml). */
+typedef struct {
+  int nz, nx, ny;
+  int npml;
+  int nt;
+  float dz, dx, dy, dt, f0;
+} EfwiGrid;
+
+/* One shot of the survey (Src_Rec.cu:74-206).  Host pointers, copied. */
+typedef struct {
+  int z_src, x_src, y_src;
+  int nrec;
+  const int *z_rec, *x_rec, *y_rec;
+  const float *win_start, *win_end; /* [nrec] seconds; windowed misfit only; may be NULL */
+  const float *weights;             /* [nrec] or NULL (all ones); windowed misfit only */
+  float src_weight;                 /* windowed misfit only */
+} EfwiShot;
+
+/* Replaces: cufd set-up (libCUFD.cu:52-91) and Cpml (Cpml.cu:7-99). */
+int efwi_create(const EfwiGrid *grid, EfwiHandle **out);
+void efwi_destroy(EfwiHandle *h);
+const char *efwi_last_error(const EfwiHandle *h);
+const char *efwi_version(void);
+
+/* Misfit windowing (para `if_win`, Parameter.cpp:146-150) and launch
+ * shape: tile_bx in {4, 8} (x rows per CTA; 0 keeps), zchunk > 0 (z planes
+ * per CTA; 0 keeps), max_batch >= 1 shots per forward launch (0 keeps). */
+int efwi_set_options(EfwiHandle *h, int if_win, int tile_bx, int zchunk, int max_batch);
+
+/* Replaces: Model (Model.cu:15-80) and the CFL check compCourantNumber
+ * (utilities.cu:186-202).  lam, mu, rho: device [nz][nx][ny]; copied. */
+int efwi_set_model(EfwiHandle *h, const float *lam, const float *mu, const float *rho,
+                   void *stream);
+
+/* Replaces: Src_Rec (Src_Rec.cu:20-249).  stf: host [nshot][nt] source
+ * time functions (untapered; the 0.001 taper of Src_Rec.cu:146 is applied
+ * here).  Shot k of later calls is shots[k]. */
+int efwi_set_survey(EfwiHandle *h, int nshot, const EfwiShot *shots, const float *stf);
+
+/* Replaces: cufd with calc_id 2 (observed data, libCUFD.cu:312-368).
+ * traces: device, concatenation over shot_ids of [3][nrec][nt]. */
+int efwi_forward(EfwiHandle *h, int n, const int *shot_ids, float *traces, void *stream);
+
+/* Replaces: cufd with calc_id 0 (misfit only, libCUFD.cu:371-420).
+ * obs: device, traces layout.  misfit: host. */
+int efwi_misfit(EfwiHandle *h, int n, const int *shot_ids, const float *obs, double *misfit,
+                void *stream);
+
+/* Replaces: cufd with calc_id 1 (misfit and gradients, libCUFD.cu:220-652).
+ * g_lam, g_mu, g_rho: device [nz][nx][ny], overwritten.  mode:
+ * EFWI_MODE_REFERENCE or EFWI_MODE_EXACT.  res (optional, device, traces
+ * layout): receives the adjoint source of each shot. */
+int efwi_gradient(EfwiHandle *h, int n, const int *shot_ids, const float *obs, int mode,
+                  double *misfit, float *g_lam, float *g_mu, float *g_rho, float *res,
+                  void *stream);
+
+/* Per-kernel timing with CUDA events on the call's stream (every
+ * `sample`-th time step; 0 disables).  efwi_profile_read fills, for each
+ * kernel class k < n, the number of timed launches, their total time in
+ * milliseconds and the total number of launches of the class, and resets
+ * the counters.  Class names: efwi_kernel_name(k). */
+int efwi_profile(EfwiHandle *h, int sample);
+int efwi_profile_read(EfwiHandle *h, int n, long long *timed, double *ms, long long *launches);
+const char *efwi_kernel_name(int k);
+int efwi_kernel_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EFWI_H_ */
