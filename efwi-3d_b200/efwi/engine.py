@@ -153,7 +153,10 @@ class Propagator:
 
     # ------------------------------------------------------------ utilities
     def trace_sizes(self, shot_ids: Sequence[int]) -> List[int]:
-        return [3 * self.shots[k].nrec * self.grid.nt for k in shot_ids]
+        # Unknown ids count as empty here; the engine rejects them with its
+        # own message (after its call-order checks).
+        return [3 * self.shots[k].nrec * self.grid.nt if 0 <= k < len(self.shots) else 0
+                for k in shot_ids]
 
     def split(self, flat: torch.Tensor, shot_ids: Sequence[int]) -> List[torch.Tensor]:
         out, off = [], 0
@@ -195,7 +198,8 @@ class Propagator:
         """Misfit and gradients w.r.t. lambda, mu, rho (device tensors)."""
         ids = self._ids(shot_ids)
         obs = _f32_dev(obs, self.device)
-        if obs.numel() != sum(self.trace_sizes(ids)):
+        if self.shots and all(0 <= k < len(self.shots) for k in ids) and \
+                obs.numel() != sum(self.trace_sizes(ids)):
             raise ValueError("observed data size does not match the shots")
         m = {"reference": _lib.MODE_REFERENCE, "exact": _lib.MODE_EXACT}[mode]
         shp = self.grid.shape

@@ -112,8 +112,7 @@ def test_multi_shot_gradient_accumulates_in_shot_order():
     obs = P.forward([0, 1, 2])
     P.set_model(torch.from_numpy(lam), torch.from_numpy(mu), torch.from_numpy(rho))
     J, gl, gm, gr = P.gradient([0, 1, 2], obs)
-    oobs = [o.astype(np.float64) for o in P.split(obs.cpu(), [0, 1, 2])]
-    oobs = [o.numpy() for o in oobs]
+    oobs = [o.numpy().astype(np.float64) for o in P.split(obs.cpu(), [0, 1, 2])]
     Jp, pl, pm, pr, _ = oracle.port().gradient(case_of(p), oobs, mode=0)
     assert abs(J - Jp) / Jp < 1e-4
     for a, b in ((gl, pl), (gm, pm), (gr, pr)):
@@ -121,19 +120,22 @@ def test_multi_shot_gradient_accumulates_in_shot_order():
 
 
 def test_config1_reduced_time_axis_against_oracle():
-    """Config-1 grid (84^3 padded) with nt = 160: traces and reference
-    gradients against the FP64 oracle."""
+    """Config-1 grid (84^3 padded, 1024 receivers) with nt = 300: traces and
+    reference gradients against the FP64 oracle.  The observed data are half
+    the true-model traces, so that the residual is not a small difference of
+    nearly equal FP32 traces (whose rounding would dominate it)."""
     from efwi import synthetic
     from efwi.engine import Propagator
-    p = synthetic.config1(nt=160)
+    p = synthetic.config1(nt=300)
     lam, mu, rho = p.params("init")
     lt, mt, rt = p.params("true")
     P = Propagator(p.grid)
     P.set_survey(p.shots, p.stf)
     P.set_model(torch.from_numpy(lt), torch.from_numpy(mt), torch.from_numpy(rt))
-    obs = P.forward([0])
-    port_obs = oracle.port().forward(case_of(p, "true"))
-    assert rel_l2(obs.cpu(), port_obs[0]) < 1e-4
+    tr = P.forward([0])
+    port_tr = oracle.port().forward(case_of(p, "true"))
+    assert rel_l2(tr.cpu(), port_tr[0]) < 1e-4
+    obs = 0.5 * tr
     P.set_model(torch.from_numpy(lam), torch.from_numpy(mu), torch.from_numpy(rho))
     J, gl, gm, gr = P.gradient([0], obs)
     Jp, pl, pm, pr, _ = oracle.port().gradient(
