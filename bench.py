@@ -47,7 +47,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nt", type=int, default=24, help="time steps of the CPU samples")
     ap.add_argument("--tile-bx", type=int, default=4)
-    ap.add_argument("--zchunk", type=int, default=16)
+    ap.add_argument("--zchunk", type=int, default=8)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     return ap.parse_args()
 
 
@@ -269,6 +270,8 @@ def main():
     torch.cuda.synchronize()
     lam, mu, rho = (torch.from_numpy(x).to(dev) for x in prob.params("init"))
     P.set_model(lam, mu, rho)
+    from efwi.autotune import autotune
+    tune = autotune(P, 0, P.split(obs, ids)[0].reshape(-1)) if a.autotune else None
 
     stream = torch.cuda.current_stream(dev)
 
@@ -382,7 +385,7 @@ def main():
                            "model_cells": a.n, "padded": g.nz, "shots_per_gpu": len(ids),
                            "nt": g.nt, "mode": "reference",
                            "l2": "inputs larger than L2 (9 fields x 14 MB per shot + shell store)",
-                           "tile_bx": a.tile_bx, "zchunk": a.zchunk},
+                           "autotune": tune},
                 "roofline": roof, "step_roofline": whole, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clocks,
                 "kernel_profile": {k: {"launches": v["launches"],

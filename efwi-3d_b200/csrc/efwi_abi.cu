@@ -8,6 +8,8 @@
 //   - forward-only calls advance up to `max_batch` shots per launch;
 //   - the reference gradient runs shot by shot with the boundary shell
 //     stored in HBM, and accumulates the images in shot order.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -75,8 +77,13 @@ struct Pending {
 struct EfwiHandle {
   EfwiGrid grid{};
   Geo geo{};
-  long long N = 0;
-  int if_win = 0, bx = 4, zchunk = 16, max_batch = 4;
+  long long N = 0;  // cells of one pitched volume
+  int py = 0;       // y pitch
+  int if_win = 0, bx = 4, zchunk = 8, max_batch = 4;
+  int variant = 1;  // 0: L1-served stencils, 1: TMA-staged planes
+  int fcfg = 0, rcfg = 0;  // launch configurations of the TMA kernels
+  int zchunk_rev = 8;      // z planes per CTA of the reverse kernels
+  int nt_limit = 0;        // > 0: time loops stop early (timing probes)
   std::string err;
 
   DevBuf coef, lam, mu, buoy;
@@ -89,7 +96,8 @@ struct EfwiHandle {
   DevBuf pts;
   int npts = 0;
 
-  DevBuf fields, psi, adj, traces_tm, res_tm, shell, partial, jdev, recbuf, winbuf, scalar;
+  DevBuf fields, psi, adj, traces_tm, res_tm, shell, partial, jdev, recbuf, winbuf, scalar, grad;
+  DevBuf status;  // pipeline status word (EFWI_STATUS_*)
 
   int prof_sample = 0;
   std::vector<cudaEvent_t> ev_pool;
@@ -181,7 +189,7 @@ void taper_stf(const float *in, int nt, float dt, float *out) {
 // [npml-2, n-npml+1]^3 minus its part more than 4 cells inside every face.
 // Points outside [2, n-3]^3 never change (they stay zero), so they are left
 // out.
-std::vector<int> shell_points(const EfwiGrid &g) {
+std::vector<int> shell_points(const EfwiGrid &g, int py) {
   std::vector<int> pts;
   const int lo = g.npml - 2;
   const int hz = g.nz - g.npml + 1, hx = g.nx - g.npml + 1, hy = g.ny - g.npml + 1;
@@ -190,7 +198,7 @@ std::vector<int> shell_points(const EfwiGrid &g) {
       for (int y = std::max(lo, 2); y <= std::min(hy, g.ny - 3); ++y) {
         const bool in = z <= lo + 4 || z >= hz - 4 || x <= lo + 4 || x >= hx - 4 ||
                         y <= lo + 4 || y >= hy - 4;
-        if (in) pts.push_back((int)(((long long)z * g.nx + x) * g.ny + y));
+        if (in) pts.push_back((int)(((long long)z * g.nx + x) * py + y));
       }
   return pts;
 }
@@ -238,6 +246,59 @@ int check_launch(EfwiHandle *h, const char *what) {
   if (e != cudaSuccess) return fail(h, EFWI_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
   return EFWI_OK;
 }
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int get_encoder(EfwiHandle *h) {
+  if (g_encode) return EFWI_OK;
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+    return fail(h, EFWI_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  return EFWI_OK;
+}
+
+// Tensor map of S stacked pitched volumes [S*nz][nx][py]; halo boxes of
+// 40 (y) x (bx + 4) (x) x 1 plane, or point boxes of 32 x bx x 1.
+int make_map(EfwiHandle *h, CUtensorMap *m, const float *base, int S, bool halo, int bx) {
+  int rc = get_encoder(h);
+  if (rc) return rc;
+  if (((uintptr_t)base & 15) != 0 || (h->py & 3) != 0)
+    return fail(h, EFWI_ERR_ARG, "tensor map base or pitch not 16-byte aligned");
+  cuuint64_t dims[3] = {(cuuint64_t)h->py, (cuuint64_t)h->grid.nx, (cuuint64_t)h->grid.nz * S};
+  cuuint64_t strides[2] = {(cuuint64_t)h->py * 4, (cuuint64_t)h->grid.nx * h->py * 4};
+  cuuint32_t box[3] = {halo ? (cuuint32_t)TMA_BOXY : 32u,
+                       (cuuint32_t)(halo ? bx + 2 * TMA_HX : bx), 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(h, EFWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return EFWI_OK;
+}
+
+// Resets the status word at the start of a call.
+int status_reset(EfwiHandle *h, cudaStream_t st) {
+  CK_CUDA(h, h->status.ensure(sizeof(int)));
+  CK_CUDA(h, cudaMemsetAsync(h->status.p, 0, sizeof(int), st));
+  return EFWI_OK;
+}
+
+// Reads the status word (synchronises the stream).
+int status_check(EfwiHandle *h, cudaStream_t st) {
+  int v = 0;
+  CK_CUDA(h, cudaMemcpyAsync(&v, h->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK_CUDA(h, cudaStreamSynchronize(st));
+  if (v != EFWI_STATUS_OK) return fail(h, EFWI_ERR_CUDA, "a bulk-copy pipeline wait timed out");
+  return EFWI_OK;
+}
+
+struct FwdMaps {
+  Maps<11> s;  // vz vx vy | szz sxx syy sxz sxy syz | lam mu
+  Maps<9> v;   // sxz syz sxx sxy syy | vz vx vy | buoy
+};
 
 Fields fields_at(float *base, long long N, int S) {
   // volumes of a batch of S shots: 9 arrays of S*N floats
@@ -326,24 +387,36 @@ int check_ready(EfwiHandle *h, int n, const int *ids) {
   return EFWI_OK;
 }
 
-dim3 stencil_grid(const EfwiHandle *h, int S, int *nzc) {
-  *nzc = (h->grid.nz + h->zchunk - 1) / h->zchunk;
-  return dim3((h->grid.ny + 31) / 32, (h->grid.nx + h->bx - 1) / h->bx, (unsigned)(S * *nzc));
+dim3 stencil_grid(const EfwiHandle *h, int S, int bx, int zchunk, int *nzc) {
+  *nzc = (h->grid.nz + zchunk - 1) / zchunk;
+  return dim3((h->grid.ny + 31) / 32, (h->grid.nx + bx - 1) / bx, (unsigned)(S * *nzc));
+}
+
+int nt_eff(const EfwiHandle *h) {
+  return h->nt_limit > 0 && h->nt_limit < h->grid.nt ? std::max(h->nt_limit, 2) : h->grid.nt;
 }
 
 // One forward time step of a batch: stress (+ source), velocity, receivers.
 int forward_step(EfwiHandle *h, Fields f, Psi ps, int S, const SrcArgs &src, const RecArgs &rec,
-                 float *traces_tm, cudaStream_t st, int it) {
+                 float *traces_tm, cudaStream_t st, int it, const FwdMaps *maps) {
   int nzc;
-  const dim3 grid = stencil_grid(h, S, &nzc);
+  const int bx = maps ? fwd_tma_tile(h->fcfg) : h->bx;
+  const dim3 grid = stencil_grid(h, S, bx, h->zchunk, &nzc);
+  int *status = h->status.as<int>();
   {
     Timer t(h, K_STRESS_FWD, st, it);
-    launch_stress_fwd(h->bx, grid, st, h->geo, f, ps, h->lam.as<float>(), h->mu.as<float>(),
-                      h->zchunk, nzc, src);
+    if (maps)
+      launch_stress_fwd_tma(h->fcfg, grid, st, maps->s, h->geo, f, ps, h->zchunk, nzc, src, status);
+    else
+      launch_stress_fwd(h->bx, grid, st, h->geo, f, ps, h->lam.as<float>(), h->mu.as<float>(),
+                        h->zchunk, nzc, src);
   }
   {
     Timer t(h, K_VELOCITY_FWD, st, it);
-    launch_velocity_fwd(h->bx, grid, st, h->geo, f, ps, h->buoy.as<float>(), h->zchunk, nzc);
+    if (maps)
+      launch_velocity_fwd_tma(h->fcfg, grid, st, maps->v, h->geo, f, ps, h->zchunk, nzc, status);
+    else
+      launch_velocity_fwd(h->bx, grid, st, h->geo, f, ps, h->buoy.as<float>(), h->zchunk, nzc);
   }
   if (rec.ncell > 0) {
     Timer t(h, K_RECORD, st, it);
@@ -385,15 +458,33 @@ int run_forward_batch(EfwiHandle *h, const int *ids, int S, float *traces_tm, lo
     CK_CUDA(h, cudaMemcpyAsync(dstf + (size_t)s * nt, h->stf.as<float>() + (size_t)ids[s] * nt,
                                sizeof(float) * nt, cudaMemcpyDeviceToDevice, st));
   SrcArgs src{dcell, dstf, nt, 0};
+  FwdMaps maps;
+  const FwdMaps *mp = nullptr;
+  if (h->variant == 1) {
+    const float *sm[11] = {f.vz, f.vx, f.vy, f.szz, f.sxx, f.syy, f.sxz, f.sxy, f.syz,
+                           h->lam.as<float>(), h->mu.as<float>()};
+    const float *vm[9] = {f.sxz, f.syz, f.sxx, f.sxy, f.syy, f.vz, f.vx, f.vy, h->buoy.as<float>()};
+    const int bxf = fwd_tma_tile(h->fcfg);
+    for (int k = 0; k < 11; ++k) {
+      rc = make_map(h, &maps.s.m[k], sm[k], k < 9 ? S : 1, k < 3, bxf);
+      if (rc) return rc;
+    }
+    for (int k = 0; k < 9; ++k) {
+      rc = make_map(h, &maps.v.m[k], vm[k], k < 8 ? S : 1, k < 5, bxf);
+      if (rc) return rc;
+    }
+    mp = &maps;
+  }
   const int npts = h->npts;
-  for (int it = 0; it <= nt - 2; ++it) {
+  const int ntl = nt_eff(h);
+  for (int it = 0; it <= ntl - 2; ++it) {
     if (shell) {
       Timer t(h, K_SHELL_SAVE, st, it);
       k_shell_save<<<(npts + 255) / 256, 256, 0, st>>>(f, h->pts.as<int>(), npts,
                                                        shell + (size_t)it * 9 * npts);
     }
     src.it = it;
-    rc = forward_step(h, f, ps, S, src, rec, traces_tm, st, it);
+    rc = forward_step(h, f, ps, S, src, rec, traces_tm, st, it, mp);
     if (rc) return rc;
   }
   return check_launch(h, "forward");
@@ -464,14 +555,15 @@ int efwi_create(const EfwiGrid *g, EfwiHandle **out) {
     return rc;
   }
   h->grid = *g;
-  h->N = (long long)g->nz * g->nx * g->ny;
+  h->py = (g->ny + 3) & ~3;
+  h->N = (long long)g->nz * g->nx * h->py;
   if (h->N >= (1LL << 31)) {
     *out = h;
     return fail(h, EFWI_ERR_ARG, "grid of %lld cells exceeds 2^31", h->N);
   }
   Geo &G = h->geo;
   G.nz = g->nz; G.nx = g->nx; G.ny = g->ny; G.np = g->npml;
-  G.N = h->N; G.sz = (long long)g->nx * g->ny; G.sx = g->ny;
+  G.N = h->N; G.sz = (long long)g->nx * h->py; G.sx = h->py;
   G.dt = g->dt; G.idz = 1.0f / g->dz; G.idx = 1.0f / g->dx; G.idy = 1.0f / g->dy;
   G.slab_z = 2LL * g->npml * g->nx * g->ny;
   G.slab_x = (long long)g->nz * 2 * g->npml * g->ny;
@@ -482,12 +574,24 @@ int efwi_create(const EfwiGrid *g, EfwiHandle **out) {
   cpml_profile(g->nz, g->npml, g->dz, g->f0, g->dt, c.data());
   cpml_profile(g->nx, g->npml, g->dx, g->f0, g->dt, c.data() + 6 * g->nz);
   cpml_profile(g->ny, g->npml, g->dy, g->f0, g->dt, c.data() + 6 * (g->nz + g->nx));
+  // The kernels multiply by 1/K and 1/K_half instead of dividing by K.
+  {
+    const int ns[3] = {g->nz, g->nx, g->ny};
+    float *row = c.data();
+    for (int ax = 0; ax < 3; ++ax) {
+      for (int i = 0; i < ns[ax]; ++i) {
+        row[CK * ns[ax] + i] = 1.0f / row[CK * ns[ax] + i];
+        row[CKH * ns[ax] + i] = 1.0f / row[CKH * ns[ax] + i];
+      }
+      row += 6 * ns[ax];
+    }
+  }
   CK_CUDA(h, h->coef.ensure(sizeof(float) * c.size()));
   CK_CUDA(h, cudaMemcpy(h->coef.p, c.data(), sizeof(float) * c.size(), cudaMemcpyHostToDevice));
   G.cz = h->coef.as<float>();
   G.cx = G.cz + 6 * g->nz;
   G.cy = G.cx + 6 * g->nx;
-  std::vector<int> pts = shell_points(*g);
+  std::vector<int> pts = shell_points(*g, h->py);
   h->npts = (int)pts.size();
   if (!pts.empty()) {
     CK_CUDA(h, h->pts.ensure(sizeof(int) * pts.size()));
@@ -513,6 +617,30 @@ int efwi_set_options(EfwiHandle *h, int if_win, int tile_bx, int zchunk, int max
   return EFWI_OK;
 }
 
+int efwi_set_tuning(EfwiHandle *h, int fwd_cfg, int zchunk_fwd, int rev_cfg, int zchunk_rev) {
+  if (!h) return EFWI_ERR_ARG;
+  if (fwd_cfg < 0 || fwd_cfg > 3 || rev_cfg < 0 || rev_cfg > 3 || zchunk_fwd < 0 || zchunk_rev < 0)
+    return fail(h, EFWI_ERR_ARG, "invalid tuning (cfg 0-3, zchunk >= 0)");
+  h->fcfg = fwd_cfg;
+  h->rcfg = rev_cfg;
+  if (zchunk_fwd) h->zchunk = zchunk_fwd;
+  if (zchunk_rev) h->zchunk_rev = zchunk_rev;
+  return EFWI_OK;
+}
+
+int efwi_set_nt_limit(EfwiHandle *h, int nt_limit) {
+  if (!h || nt_limit < 0) return EFWI_ERR_ARG;
+  h->nt_limit = nt_limit;
+  return EFWI_OK;
+}
+
+int efwi_set_variant(EfwiHandle *h, int variant) {
+  if (!h) return EFWI_ERR_ARG;
+  if (variant != 0 && variant != 1) return fail(h, EFWI_ERR_ARG, "variant must be 0 or 1");
+  h->variant = variant;
+  return EFWI_OK;
+}
+
 int efwi_set_model(EfwiHandle *h, const float *lam, const float *mu, const float *rho, void *stream) {
   if (!h) return EFWI_ERR_ARG;
   if (!lam || !mu || !rho) return fail(h, EFWI_ERR_ARG, "null model pointer");
@@ -521,15 +649,17 @@ int efwi_set_model(EfwiHandle *h, const float *lam, const float *mu, const float
   CK_CUDA(h, h->lam.ensure(bytes));
   CK_CUDA(h, h->mu.ensure(bytes));
   CK_CUDA(h, h->buoy.ensure(bytes));
-  CK_CUDA(h, cudaMemcpyAsync(h->lam.p, lam, bytes, cudaMemcpyDeviceToDevice, st));
-  CK_CUDA(h, cudaMemcpyAsync(h->mu.p, mu, bytes, cudaMemcpyDeviceToDevice, st));
-  k_prep_buoyancy<<<1184, 256, 0, st>>>(rho, h->buoy.as<float>(), h->grid.nz, h->grid.nx, h->grid.ny);
-  h->launches[K_OTHER]++;
+  const EfwiGrid &G = h->grid;
+  k_pitch_copy<<<1184, 256, 0, st>>>(lam, h->lam.as<float>(), G.nz, G.nx, G.ny, h->py, 1);
+  k_pitch_copy<<<1184, 256, 0, st>>>(mu, h->mu.as<float>(), G.nz, G.nx, G.ny, h->py, 1);
+  CK_CUDA(h, cudaMemsetAsync(h->buoy.p, 0, bytes, st));
+  k_prep_buoyancy<<<1184, 256, 0, st>>>(rho, h->buoy.as<float>(), G.nz, G.nx, G.ny, h->py);
+  h->launches[K_OTHER] += 3;
   // CFL check of the reference (2D formula with min(dz, dx)).
   CK_CUDA(h, h->jdev.ensure(64));
   unsigned int *vmax = (unsigned int *)h->jdev.p;
   CK_CUDA(h, cudaMemsetAsync(vmax, 0, sizeof(unsigned int), st));
-  k_max_vp<<<592, 256, 0, st>>>(lam, mu, rho, h->N, vmax);
+  k_max_vp<<<592, 256, 0, st>>>(lam, mu, rho, (long long)G.nz * G.nx * G.ny, vmax);
   h->launches[K_OTHER]++;
   int rc = check_launch(h, "set_model");
   if (rc) return rc;
@@ -560,14 +690,14 @@ int efwi_set_survey(EfwiHandle *h, int nshot, const EfwiShot *shots, const float
     if (s.nrec < 0 || (s.nrec > 0 && (!s.z_rec || !s.x_rec || !s.y_rec)))
       return fail(h, EFWI_ERR_ARG, "shot %d: invalid receivers", k);
     ShotHost &o = out[k];
-    o.src_cell = ((long long)s.z_src * g.nx + s.x_src) * g.ny + s.y_src;
+    o.src_cell = ((long long)s.z_src * g.nx + s.x_src) * h->py + s.y_src;
     o.nrec = s.nrec;
     o.rec_cell.resize(s.nrec);
     for (int r = 0; r < s.nrec; ++r) {
       const int z = s.z_rec[r], x = s.x_rec[r], y = s.y_rec[r];
       if (z < 0 || z >= g.nz || x < 0 || x >= g.nx || y < 0 || y >= g.ny)
         return fail(h, EFWI_ERR_ARG, "shot %d receiver %d at (%d, %d, %d) outside the grid", k, r, z, x, y);
-      o.rec_cell[r] = ((long long)z * g.nx + x) * g.ny + y;
+      o.rec_cell[r] = ((long long)z * g.nx + x) * h->py + y;
     }
     o.win0.assign(s.nrec, 0.f);
     o.win1.assign(s.nrec, 0.f);
@@ -597,6 +727,8 @@ int efwi_forward(EfwiHandle *h, int n, const int *ids, float *traces, void *stre
   cudaStream_t st = (cudaStream_t)stream;
   const int nt = h->grid.nt;
   long long out_off = 0;
+  rc = status_reset(h, st);
+  if (rc) return rc;
   for (int b0 = 0; b0 < n; b0 += h->max_batch) {
     const int S = std::min(h->max_batch, n - b0);
     long long ntr = 0;
@@ -618,7 +750,7 @@ int efwi_forward(EfwiHandle *h, int n, const int *ids, float *traces, void *stre
     rc = check_launch(h, "traces");
     if (rc) return rc;
   }
-  return EFWI_OK;
+  return status_check(h, st);
 }
 
 static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs, int mode,
@@ -627,10 +759,18 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
   const int nt = h->grid.nt;
   const long long N = h->N;
   const bool grad = glam != nullptr;
+  {
+    int rc0 = status_reset(h, st);
+    if (rc0) return rc0;
+  }
+  float *out_lam = glam, *out_mu = gmu, *out_rho = grho;
   if (grad) {
-    CK_CUDA(h, cudaMemsetAsync(glam, 0, sizeof(float) * N, st));
-    CK_CUDA(h, cudaMemsetAsync(gmu, 0, sizeof(float) * N, st));
-    CK_CUDA(h, cudaMemsetAsync(grho, 0, sizeof(float) * N, st));
+    // images accumulate in pitched volumes, copied out at the end
+    CK_CUDA(h, h->grad.ensure(sizeof(float) * 3 * N));
+    CK_CUDA(h, cudaMemsetAsync(h->grad.p, 0, sizeof(float) * 3 * N, st));
+    glam = h->grad.as<float>();
+    gmu = glam + N;
+    grho = glam + 2 * N;
   }
   CK_CUDA(h, h->jdev.ensure(sizeof(double) * (n + 8)));
   double *jdev = h->jdev.as<double>() + 1;
@@ -667,20 +807,51 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     long long *dcell = h->scalar.as<long long>();
     float *dstf = (float *)((char *)h->scalar.p + 256);
     SrcArgs src{dcell, dstf, nt, 0};
-    int nzc;
-    const dim3 grid = stencil_grid(h, 1, &nzc);
     const int npts = h->npts;
     const float *shell = h->shell.as<float>();
+    // Reverse kernels: TMA-staged (tile 32 x 4) or L1-served.
+    Maps<21> m1;
+    Maps<23> m2;
+    const bool tma = h->variant == 1;
+    const EfwiGrid &G = h->grid;
+    if (tma) {
+      const float *h1[11] = {f.sxz, f.syz, f.sxx, f.sxy, f.syy, a.sxz, a.syz, a.sxx, a.sxy, a.syy, a.szz};
+      const float *p1[10] = {f.vz, f.vx, f.vy, a.vz, a.vx, a.vy, h->buoy.as<float>(),
+                             h->lam.as<float>(), h->mu.as<float>(), grho};
+      const float *h2[6] = {f.vz, f.vx, f.vy, a.vz, a.vx, a.vy};
+      const float *p2[17] = {f.szz, f.sxx, f.syy, f.sxz, f.sxy, f.syz, a.szz, a.sxx, a.syy,
+                             a.sxz, a.sxy, a.syz, h->lam.as<float>(), h->mu.as<float>(),
+                             h->buoy.as<float>(), glam, gmu};
+      for (int k2 = 0; k2 < 21 && rc == 0; ++k2)
+        rc = make_map(h, &m1.m[k2], k2 < 11 ? h1[k2] : p1[k2 - 11], 1, k2 < 11, 4);
+      for (int k2 = 0; k2 < 23 && rc == 0; ++k2)
+        rc = make_map(h, &m2.m[k2], k2 < 6 ? h2[k2] : p2[k2 - 6], 1, k2 < 6, 4);
+      if (rc) return rc;
+    }
+    int nzc;
+    const int bxr = tma ? 4 : h->bx;
+    const int zcr = tma ? h->zchunk_rev : h->zchunk;
+    const dim3 grid = stencil_grid(h, 1, bxr, zcr, &nzc);
+    (void)G;
+    int *status = h->status.as<int>();
     auto K1 = [&](int rev, int adj, int it) {
       Timer t(h, K_REV_VELOCITY, st, it);
-      launch_rev_velocity(h->bx, grid, st, h->geo, f, a, ps, h->lam.as<float>(),
-                          h->mu.as<float>(), h->buoy.as<float>(), grho, h->zchunk, nzc, rev, adj);
+      if (tma)
+        launch_rev_velocity_tma(h->rcfg, grid, st, m1, h->geo, f, a, ps, grho, zcr, nzc, rev, adj,
+                                status);
+      else
+        launch_rev_velocity(h->bx, grid, st, h->geo, f, a, ps, h->lam.as<float>(),
+                            h->mu.as<float>(), h->buoy.as<float>(), grho, zcr, nzc, rev, adj);
     };
     auto K2 = [&](int rev, int adj, int it) {
       Timer t(h, K_REV_STRESS, st, it);
       src.it = it;
-      launch_rev_stress(h->bx, grid, st, h->geo, f, a, ps, h->lam.as<float>(), h->mu.as<float>(),
-                        h->buoy.as<float>(), glam, gmu, h->zchunk, nzc, rev, adj, src);
+      if (tma)
+        launch_rev_stress_tma(h->rcfg, grid, st, m2, h->geo, f, a, ps, glam, gmu, zcr, nzc, rev,
+                              adj, src, status);
+      else
+        launch_rev_stress(h->bx, grid, st, h->geo, f, a, ps, h->lam.as<float>(), h->mu.as<float>(),
+                          h->buoy.as<float>(), glam, gmu, zcr, nzc, rev, adj, src);
     };
     auto inject = [&](int it) {
       if (rec.ncell == 0) return;
@@ -692,10 +863,11 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
       Timer t(h, K_SHELL_RESTORE, st, it);
       k_shell_restore<<<(npts + 255) / 256, 256, 0, st>>>(f, h->pts.as<int>(), npts, shell + (size_t)it * 9 * npts, stress);
     };
-    K1(0, 1, nt - 1);
-    inject(nt - 1);
-    K2(0, 1, nt - 1);
-    for (int it = nt - 2; it >= 0; --it) {
+    const int ntl = nt_eff(h);
+    K1(0, 1, ntl - 1);
+    inject(ntl - 1);
+    K2(0, 1, ntl - 1);
+    for (int it = ntl - 2; it >= 0; --it) {
       const int adj = it > 0;  // the adjoint update of step 0 feeds no image
       K1(1, adj, it);
       if (adj) inject(it);
@@ -706,12 +878,25 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     rc = check_launch(h, "reverse");
     if (rc) return rc;
   }
+  if (grad) {
+    const EfwiGrid &G = h->grid;
+    k_pitch_copy<<<1184, 256, 0, st>>>(glam, out_lam, G.nz, G.nx, G.ny, h->py, 0);
+    k_pitch_copy<<<1184, 256, 0, st>>>(gmu, out_mu, G.nz, G.nx, G.ny, h->py, 0);
+    k_pitch_copy<<<1184, 256, 0, st>>>(grho, out_rho, G.nz, G.nx, G.ny, h->py, 0);
+    h->launches[K_OTHER] += 3;
+    int rc = check_launch(h, "gradient copy-out");
+    if (rc) return rc;
+  }
   std::vector<double> js(std::max(n, 1), 0.0);
   if (n > 0) CK_CUDA(h, cudaMemcpyAsync(js.data(), jdev, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   CK_CUDA(h, cudaStreamSynchronize(st));
   double J = 0.0;
   for (int k = 0; k < n; ++k) J += js[k];
   if (misfit) *misfit = J;
+  {
+    int rc1 = status_check(h, st);
+    if (rc1) return rc1;
+  }
   if (h->prof_sample > 0) return resolve_profile(h);
   return EFWI_OK;
 }

@@ -9,15 +9,31 @@ namespace efwi {
 // Buoyancy 1/rho on [2, n-3]^3 and 1/1000 elsewhere (Model.cu:65,76 with
 // aveBycInit, utilities.cu:117-128).  The reciprocal is formed in double as
 // the reference does.
-__global__ void k_prep_buoyancy(const float *rho, float *buoy, int nz, int nx, int ny) {
+// rho is in the caller's [nz][nx][ny] layout; buoy has the y pitch py.
+__global__ void k_prep_buoyancy(const float *rho, float *buoy, int nz, int nx, int ny, int py) {
   const long long n = (long long)nz * nx * ny;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const int y = (int)(i % ny);
-    const int x = (int)((i / ny) % nx);
-    const int z = (int)(i / ((long long)nx * ny));
+    const long long zx = i / ny;
+    const int x = (int)(zx % nx);
+    const int z = (int)(zx / nx);
     const bool in = z >= 2 && z <= nz - 3 && x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3;
-    buoy[i] = in ? (float)(1.0 / (double)rho[i]) : (float)(1.0 / 1000.0);
+    buoy[zx * py + y] = in ? (float)(1.0 / (double)rho[i]) : (float)(1.0 / 1000.0);
+  }
+}
+
+// Copies between the caller's [nz][nx][ny] volumes and pitched ones;
+// `to_pitched` selects the direction.  The pad columns are zeroed.
+__global__ void k_pitch_copy(const float *src, float *dst, int nz, int nx, int ny, int py,
+                             int to_pitched) {
+  const long long n = (long long)nz * nx * py;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % py);
+    const long long zx = i / py;
+    if (to_pitched) dst[i] = (y < ny) ? src[zx * ny + y] : 0.0f;
+    else if (y < ny) dst[zx * ny + y] = src[i];
   }
 }
 

@@ -1,9 +1,11 @@
 // Shared device-side definitions of the B200 elastic propagation engine.
 //
-// Layout (HBM): every volume is [nz][nx][ny] float32, y fastest -- the
-// torch-native C order of the caller's tensors, so no transposes are made
-// (the reference transposes to z-fastest on the host, libCUFD.cu:72-80).
-// Shots of one batch are stacked with stride N = nz*nx*ny.
+// Layout (HBM): every volume is [nz][nx][py] float32, y fastest -- the
+// torch-native C order of the caller's tensors (the reference transposes to
+// z-fastest on the host, libCUFD.cu:72-80), with the y pitch py = ny rounded
+// up to a multiple of 4 so that every row starts on a 16-byte boundary (the
+// alignment of bulk tensor copies).  Shots of one batch are stacked with
+// stride N = nz*nx*py.
 //
 // C-PML memory variables live only in their slabs (the reference keeps 18
 // full-grid arrays, libCUFD.cu:173-191):
@@ -31,15 +33,17 @@ namespace efwi {
 // y: 0 vy_y 1 vz_y 2 vx_y 3 syy_y 4 syz_y 5 sxy_y
 enum { PSI_VA = 0, PSI_VB1 = 1, PSI_VB2 = 2, PSI_SAA = 3, PSI_SAB1 = 4, PSI_SAB2 = 5 };
 
-// Coefficient rows of one axis profile [6][n]: K, a, b, K_half, a_half, b_half
-// (utilities.cu:204-320).
+// Coefficient rows of one axis profile [6][n]: 1/K, a, b, 1/K_half, a_half,
+// b_half (utilities.cu:204-320).  The reference divides by K; the kernels
+// multiply by the stored reciprocal (a rounding difference of at most one
+// unit in the last place).
 enum { CK = 0, CA = 1, CB = 2, CKH = 3, CAH = 4, CBH = 5 };
 
 struct Geo {
   int nz, nx, ny, np;
-  long long N;      // cells per volume
-  long long sz;     // z stride = nx*ny
-  int sx;           // x stride = ny
+  long long N;      // cells per volume (with the y pitch)
+  long long sz;     // z stride = nx*py
+  int sx;           // x stride = py, the y pitch
   float dt, idz, idx, idy;
   long long slab_z, slab_x, slab_y;  // elements per variable of each slab
   const float *cz, *cx, *cy;         // [6][n] coefficient rows
@@ -52,6 +56,10 @@ struct Fields {
 struct Psi {
   float *z, *x, *y;  // [6][slab] per axis
 };
+
+__device__ __forceinline__ long long cell(const Geo &g, int z, int x, int y) {
+  return ((long long)z * g.nx + x) * g.sx + y;
+}
 
 __device__ __forceinline__ float dminus(float m2, float m1, float p0, float p1) {
   // c1 (f[i] - f[i-1]) - c2 (f[i+1] - f[i-2])

@@ -57,7 +57,7 @@ k_stress_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ lam,
   const long long src_cell = src.cell ? src.cell[shot] : -1;
   const float src_amp = src.stf ? src.stf[(long long)shot * src.nt + src.it] : 0.f;
 
-  long long i = ((long long)z0 * nx + x) * ny + y;
+  long long i = ((long long)z0 * nx + x) * sx + y;
   // z queues: vz needs z-2..z+1 (D-), vx and vy need z-1..z+2 (D+).
   float qz0 = vz[i - 2 * sz], qz1 = vz[i - sz], qz2 = vz[i], qz3 = vz[i + sz];
   float qx0 = vx[i - sz], qx1 = vx[i], qx2 = vx[i + sz], qx3 = vx[i + 2 * sz];
@@ -81,31 +81,31 @@ k_stress_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ lam,
       const long long k = psi_z_idx(g, z, x, y);
       float m;
       m = bz * pzb[PSI_VA * g.slab_z + k] + az * ezz;
-      pzb[PSI_VA * g.slab_z + k] = m; ezz = ezz / Kz + m;
+      pzb[PSI_VA * g.slab_z + k] = m; ezz = ezz * Kz + m;
       m = bzh * pzb[PSI_VB1 * g.slab_z + k] + azh * dvx_dz;
-      pzb[PSI_VB1 * g.slab_z + k] = m; dvx_dz = dvx_dz / Kzh + m;
+      pzb[PSI_VB1 * g.slab_z + k] = m; dvx_dz = dvx_dz * Kzh + m;
       m = bzh * pzb[PSI_VB2 * g.slab_z + k] + azh * dvy_dz;
-      pzb[PSI_VB2 * g.slab_z + k] = m; dvy_dz = dvy_dz / Kzh + m;
+      pzb[PSI_VB2 * g.slab_z + k] = m; dvy_dz = dvy_dz * Kzh + m;
     }
     if (xs) {
       const long long k = psi_x_idx(g, z, x, y);
       float m;
       m = bx * pxb[PSI_VA * g.slab_x + k] + ax * exx;
-      pxb[PSI_VA * g.slab_x + k] = m; exx = exx / Kx + m;
+      pxb[PSI_VA * g.slab_x + k] = m; exx = exx * Kx + m;
       m = bxh * pxb[PSI_VB1 * g.slab_x + k] + axh * dvz_dx;
-      pxb[PSI_VB1 * g.slab_x + k] = m; dvz_dx = dvz_dx / Kxh + m;
+      pxb[PSI_VB1 * g.slab_x + k] = m; dvz_dx = dvz_dx * Kxh + m;
       m = bxh * pxb[PSI_VB2 * g.slab_x + k] + axh * dvy_dx;
-      pxb[PSI_VB2 * g.slab_x + k] = m; dvy_dx = dvy_dx / Kxh + m;
+      pxb[PSI_VB2 * g.slab_x + k] = m; dvy_dx = dvy_dx * Kxh + m;
     }
     if (ys) {
       const long long k = psi_y_idx(g, z, x, y);
       float m;
       m = by * pyb[PSI_VA * g.slab_y + k] + ay * eyy;
-      pyb[PSI_VA * g.slab_y + k] = m; eyy = eyy / Ky + m;
+      pyb[PSI_VA * g.slab_y + k] = m; eyy = eyy * Ky + m;
       m = byh * pyb[PSI_VB1 * g.slab_y + k] + ayh * dvz_dy;
-      pyb[PSI_VB1 * g.slab_y + k] = m; dvz_dy = dvz_dy / Kyh + m;
+      pyb[PSI_VB1 * g.slab_y + k] = m; dvz_dy = dvz_dy * Kyh + m;
       m = byh * pyb[PSI_VB2 * g.slab_y + k] + ayh * dvx_dy;
-      pyb[PSI_VB2 * g.slab_y + k] = m; dvx_dy = dvx_dy / Kyh + m;
+      pyb[PSI_VB2 * g.slab_y + k] = m; dvx_dy = dvx_dy * Kyh + m;
     }
 
     const float l = lam[i], u = mu[i], l2u = l + 2.0f * u;
@@ -176,7 +176,7 @@ k_velocity_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ buoy, int zchu
     Kyh = g.cy[CKH * ny + y]; ayh = g.cy[CAH * ny + y]; byh = g.cy[CBH * ny + y];
   }
 
-  long long i = ((long long)z0 * nx + x) * ny + y;
+  long long i = ((long long)z0 * nx + x) * sx + y;
   // z queues: szz needs z-1..z+2 (D+), sxz and syz need z-2..z+1 (D-).
   float qa0 = szz[i - sz], qa1 = szz[i], qa2 = szz[i + sz], qa3 = szz[i + 2 * sz];
   float qb0 = sxz[i - 2 * sz], qb1 = sxz[i - sz], qb2 = sxz[i], qb3 = sxz[i + sz];
@@ -204,31 +204,31 @@ k_velocity_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ buoy, int zchu
       const long long k = psi_z_idx(g, z, x, y);
       float m;
       m = bzh * pzb[PSI_SAA * g.slab_z + k] + azh * dszz_dz;
-      pzb[PSI_SAA * g.slab_z + k] = m; dszz_dz = dszz_dz / Kzh + m;
+      pzb[PSI_SAA * g.slab_z + k] = m; dszz_dz = dszz_dz * Kzh + m;
       m = bz * pzb[PSI_SAB1 * g.slab_z + k] + az * dsxz_dz;
-      pzb[PSI_SAB1 * g.slab_z + k] = m; dsxz_dz = dsxz_dz / Kz + m;
+      pzb[PSI_SAB1 * g.slab_z + k] = m; dsxz_dz = dsxz_dz * Kz + m;
       m = bz * pzb[PSI_SAB2 * g.slab_z + k] + az * dsyz_dz;
-      pzb[PSI_SAB2 * g.slab_z + k] = m; dsyz_dz = dsyz_dz / Kz + m;
+      pzb[PSI_SAB2 * g.slab_z + k] = m; dsyz_dz = dsyz_dz * Kz + m;
     }
     if (xs) {
       const long long k = psi_x_idx(g, z, x, y);
       float m;
       m = bx * pxb[PSI_SAB1 * g.slab_x + k] + ax * dsxz_dx;
-      pxb[PSI_SAB1 * g.slab_x + k] = m; dsxz_dx = dsxz_dx / Kx + m;
+      pxb[PSI_SAB1 * g.slab_x + k] = m; dsxz_dx = dsxz_dx * Kx + m;
       m = bxh * pxb[PSI_SAA * g.slab_x + k] + axh * dsxx_dx;
-      pxb[PSI_SAA * g.slab_x + k] = m; dsxx_dx = dsxx_dx / Kxh + m;
+      pxb[PSI_SAA * g.slab_x + k] = m; dsxx_dx = dsxx_dx * Kxh + m;
       m = bx * pxb[PSI_SAB2 * g.slab_x + k] + ax * dsxy_dx;
-      pxb[PSI_SAB2 * g.slab_x + k] = m; dsxy_dx = dsxy_dx / Kx + m;
+      pxb[PSI_SAB2 * g.slab_x + k] = m; dsxy_dx = dsxy_dx * Kx + m;
     }
     if (ys) {
       const long long k = psi_y_idx(g, z, x, y);
       float m;
       m = by * pyb[PSI_SAB1 * g.slab_y + k] + ay * dsyz_dy;
-      pyb[PSI_SAB1 * g.slab_y + k] = m; dsyz_dy = dsyz_dy / Ky + m;
+      pyb[PSI_SAB1 * g.slab_y + k] = m; dsyz_dy = dsyz_dy * Ky + m;
       m = by * pyb[PSI_SAB2 * g.slab_y + k] + ay * dsxy_dy;
-      pyb[PSI_SAB2 * g.slab_y + k] = m; dsxy_dy = dsxy_dy / Ky + m;
+      pyb[PSI_SAB2 * g.slab_y + k] = m; dsxy_dy = dsxy_dy * Ky + m;
       m = byh * pyb[PSI_SAA * g.slab_y + k] + ayh * dsyy_dy;
-      pyb[PSI_SAA * g.slab_y + k] = m; dsyy_dy = dsyy_dy / Kyh + m;
+      pyb[PSI_SAA * g.slab_y + k] = m; dsyy_dy = dsyy_dy * Kyh + m;
     }
 
     vz[i] = vz[i] + (dszz_dz + dsxz_dx + dsyz_dy) * b * dt;

@@ -1,6 +1,7 @@
 // Kernel declarations shared by the kernel translation units and the C-ABI.
 #pragma once
 #include "efwi_common.cuh"
+#include "efwi_tma.cuh"
 
 namespace efwi {
 
@@ -47,7 +48,37 @@ void launch_rev_stress(int bx, dim3 grid, cudaStream_t st, const Geo &g, const F
                        const float *buoy, float *glam, float *gmu, int zchunk, int nzc,
                        int do_rev, int do_adj, const SrcArgs &src);
 
-__global__ void k_prep_buoyancy(const float *rho, float *buoy, int nz, int nx, int ny);
+// TMA-staged variants (efwi_fwd_tma.cu); `status` receives
+// EFWI_STATUS_TIMEOUT if a pipeline wait ran out of time.
+// cfg selects (tile, ring depth, min CTAs/SM); fwd_tma_tile(cfg) is the
+// tile's x extent.
+int fwd_tma_tile(int cfg);
+// K_S maps: halo vz vx vy | point szz sxx syy sxz sxy syz | model lambda mu.
+void launch_stress_fwd_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<11> &maps,
+                           const Geo &g, const Fields &f, const Psi &ps, int zchunk, int nzc,
+                           const SrcArgs &src, int *status);
+// K_V maps: halo sxz syz sxx sxy syy | point vz vx vy | model buoyancy.
+void launch_velocity_fwd_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<9> &maps,
+                             const Geo &g, const Fields &f, const Psi &ps, int zchunk, int nzc,
+                             int *status);
+
+// Reverse sweep with TMA-staged planes (efwi_rev_tma.cu), tile 32 x 4.
+// K1 maps: halo sxz syz sxx sxy syy asxz asyz asxx asxy asyy aszz |
+//          point vz vx vy avz avx avy | model buoyancy lambda mu grho.
+void launch_rev_velocity_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<21> &maps,
+                             const Geo &g, const Fields &f, const Fields &a, const Psi &ps,
+                             float *grho, int zchunk, int nzc, int do_rev, int do_adj,
+                             int *status);
+// K2 maps: halo vz vx vy avz avx avy | point szz sxx syy sxz sxy syz aszz
+//          asxx asyy asxz asxy asyz | model lambda mu buoyancy glam gmu.
+void launch_rev_stress_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<23> &maps,
+                           const Geo &g, const Fields &f, const Fields &a, const Psi &ps,
+                           float *glam, float *gmu, int zchunk, int nzc, int do_rev, int do_adj,
+                           const SrcArgs &src, int *status);
+
+__global__ void k_prep_buoyancy(const float *rho, float *buoy, int nz, int nx, int ny, int py);
+__global__ void k_pitch_copy(const float *src, float *dst, int nz, int nx, int ny, int py,
+                             int to_pitched);
 __global__ void k_record(Fields f, long long N, RecArgs rec, float *traces_tm, int it);
 __global__ void k_inject(Fields a, long long N, RecArgs rec, const float *res_tm, int it);
 __global__ void k_shell_save(Fields f, const int *pts, int npts, float *dst);

@@ -98,7 +98,7 @@ k_rev_velocity(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
   float *pz = ps.z, *px = ps.x, *py = ps.y;
 
   for (int z = z0; z < z1; ++z) {
-    const long long i = ((long long)z * nx + x) * ny + y;
+    const long long i = ((long long)z * nx + x) * sx + y;
     const float b = buoy[i];
     const float avz0 = a.vz[i], avx0 = a.vx[i], avy0 = a.vy[i];
     if (do_rev && xin && yin && z >= np && z <= nz - 1 - np) {
@@ -128,8 +128,8 @@ k_rev_velocity(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
       const float dsyy_dx = -dplus(asyy[i - sx], asyy[i], asyy[i + sx], asyy[i + 2 * sx]) * idx;
       const float dsxz_dz = -dminus(asxz[i - 2 * sz], asxz[i - sz], asxz[i], asxz[i + sz]) * idz;
       const float dsxy_dy = -dminus(asxy[i - 2], asxy[i - 1], asxy[i], asxy[i + 1]) * idy;
-      float acc = l2u * dsxx_dx / cx.K * dt + l * dszz_dx / cx.K * dt + l * dsyy_dx / cx.K * dt +
-                  u / cz.Kh * dsxz_dz * dt + u / cy.Kh * dsxy_dy * dt;
+      float acc = l2u * dsxx_dx * cx.K * dt + l * dszz_dx * cx.K * dt + l * dsyy_dx * cx.K * dt +
+                  u * cz.Kh * dsxz_dz * dt + u * cy.Kh * dsxy_dy * dt;
       if (xs) acc += cx.a * (nxp(g, psx + PSI_VA * g.slab_x, z, x, y) * idx);
       if (zs) acc += cz.ah * (nzm(g, psz + PSI_VB1 * g.slab_z, z, x, y) * idz);
       if (ys) acc += cy.ah * (nym(g, psy + PSI_VB2 * g.slab_y, z, x, y) * idy);
@@ -146,8 +146,8 @@ k_rev_velocity(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
       const float dsyy_dz = -dplus(asyy[i - sz], asyy[i], asyy[i + sz], asyy[i + 2 * sz]) * idz;
       const float dsxz_dx = -dminus(asxz[i - 2 * sx], asxz[i - sx], asxz[i], asxz[i + sx]) * idx;
       const float dsyz_dy = -dminus(asyz[i - 2], asyz[i - 1], asyz[i], asyz[i + 1]) * idy;
-      float acc = l2u * dszz_dz / cz.K * dt + l * dsxx_dz / cz.K * dt + l * dsyy_dz / cz.K * dt +
-                  u / cy.Kh * dsyz_dy * dt + u / cx.Kh * dsxz_dx * dt;
+      float acc = l2u * dszz_dz * cz.K * dt + l * dsxx_dz * cz.K * dt + l * dsyy_dz * cz.K * dt +
+                  u * cy.Kh * dsyz_dy * dt + u * cx.Kh * dsxz_dx * dt;
       if (zs) acc += cz.a * (nzp(g, psz + PSI_VA * g.slab_z, z, x, y) * idz);
       if (ys) acc += cy.ah * (nym(g, psy + PSI_VB1 * g.slab_y, z, x, y) * idy);
       if (xs) acc += cx.ah * (nxm(g, psx + PSI_VB1 * g.slab_x, z, x, y) * idx);
@@ -164,8 +164,8 @@ k_rev_velocity(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
       const float dszz_dy = -dplus(aszz[i - 1], aszz[i], aszz[i + 1], aszz[i + 2]) * idy;
       const float dsxy_dx = -dminus(asxy[i - 2 * sx], asxy[i - sx], asxy[i], asxy[i + sx]) * idx;
       const float dsyz_dz = -dminus(asyz[i - 2 * sz], asyz[i - sz], asyz[i], asyz[i + sz]) * idz;
-      float acc = l2u * dsyy_dy / cy.K * dt + l * dsxx_dy / cy.K * dt + l * dszz_dy / cy.K * dt +
-                  u / cx.Kh * dsxy_dx * dt + u / cz.Kh * dsyz_dz * dt;
+      float acc = l2u * dsyy_dy * cy.K * dt + l * dsxx_dy * cy.K * dt + l * dszz_dy * cy.K * dt +
+                  u * cx.Kh * dsxy_dx * dt + u * cz.Kh * dsyz_dz * dt;
       if (ys) acc += cy.a * (nyp(g, psy + PSI_VA * g.slab_y, z, x, y) * idy);
       if (xs) acc += cx.ah * (nxm(g, psx + PSI_VB2 * g.slab_x, z, x, y) * idx);
       if (zs) acc += cz.ah * (nzm(g, psz + PSI_VB2 * g.slab_z, z, x, y) * idz);
@@ -210,7 +210,7 @@ k_rev_stress(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
   float *pz = ps.z, *px = ps.x, *py = ps.y;
 
   for (int z = z0; z < z1; ++z) {
-    const long long i = ((long long)z * nx + x) * ny + y;
+    const long long i = ((long long)z * nx + x) * sx + y;
     const float l = lam[i], u = mu[i], l2u = l + 2.0f * u;
     const float azz0 = a.szz[i], axx0 = a.sxx[i], ayy0 = a.syy[i];
     const float axz0 = a.sxz[i], axy0 = a.sxy[i], ayz0 = a.syz[i];
@@ -253,7 +253,7 @@ k_rev_stress(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
     {
       const float dvz_dx = -dplus(avz[i - sx], avz[i], avz[i + sx], avz[i + 2 * sx]) * idx;
       const float dvx_dz = -dplus(avx[i - sz], avx[i], avx[i + sz], avx[i + 2 * sz]) * idz;
-      float acc = dvz_dx / cx.K * b * dt + dvx_dz / cz.K * b * dt;
+      float acc = dvz_dx * cx.K * b * dt + dvx_dz * cz.K * b * dt;
       if (xs) acc += cx.a * (nxp(g, psx + PSI_SAB1 * g.slab_x, z, x, y) * idx);
       if (zs) acc += cz.a * (nzp(g, psz + PSI_SAB1 * g.slab_z, z, x, y) * idz);
       const float s = axz0 + acc;
@@ -265,7 +265,7 @@ k_rev_stress(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
     {
       const float dvy_dx = -dplus(avy[i - sx], avy[i], avy[i + sx], avy[i + 2 * sx]) * idx;
       const float dvx_dy = -dplus(avx[i - 1], avx[i], avx[i + 1], avx[i + 2]) * idy;
-      float acc = dvy_dx / cx.K * b * dt + dvx_dy / cy.K * b * dt;
+      float acc = dvy_dx * cx.K * b * dt + dvx_dy * cy.K * b * dt;
       if (xs) acc += cx.a * (nxp(g, psx + PSI_SAB2 * g.slab_x, z, x, y) * idx);
       if (ys) acc += cy.a * (nyp(g, psy + PSI_SAB2 * g.slab_y, z, x, y) * idy);
       const float s = axy0 + acc;
@@ -277,7 +277,7 @@ k_rev_stress(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
     {
       const float dvz_dy = -dplus(avz[i - 1], avz[i], avz[i + 1], avz[i + 2]) * idy;
       const float dvy_dz = -dplus(avy[i - sz], avy[i], avy[i + sz], avy[i + 2 * sz]) * idz;
-      float acc = dvz_dy / cy.K * b * dt + dvy_dz / cz.K * b * dt;
+      float acc = dvz_dy * cy.K * b * dt + dvy_dz * cz.K * b * dt;
       if (ys) acc += cy.a * (nyp(g, psy + PSI_SAB1 * g.slab_y, z, x, y) * idy);
       if (zs) acc += cz.a * (nzp(g, psz + PSI_SAB2 * g.slab_z, z, x, y) * idz);
       const float s = ayz0 + acc;
@@ -290,9 +290,9 @@ k_rev_stress(Geo g, Fields f, Fields a, Psi ps, const float *__restrict__ lam,
       const float dvx_dx = -dminus(avx[i - 2 * sx], avx[i - sx], avx[i], avx[i + sx]) * idx;
       const float dvz_dz = -dminus(avz[i - 2 * sz], avz[i - sz], avz[i], avz[i + sz]) * idz;
       const float dvy_dy = -dminus(avy[i - 2], avy[i - 1], avy[i], avy[i + 1]) * idy;
-      float sxx = axx0 + b * dvx_dx / cx.Kh * dt;
-      float szz = azz0 + b * dvz_dz / cz.Kh * dt;
-      float syy = ayy0 + b * dvy_dy / cy.Kh * dt;
+      float sxx = axx0 + b * dvx_dx * cx.Kh * dt;
+      float szz = azz0 + b * dvz_dz * cz.Kh * dt;
+      float syy = ayy0 + b * dvy_dy * cy.Kh * dt;
       if (xs) sxx += cx.ah * (nxm(g, psx + PSI_SAA * g.slab_x, z, x, y) * idx);
       if (zs) szz += cz.ah * (nzm(g, psz + PSI_SAA * g.slab_z, z, x, y) * idz);
       if (ys) syy += cy.ah * (nym(g, psy + PSI_SAA * g.slab_y, z, x, y) * idy);

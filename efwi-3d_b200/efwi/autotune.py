@@ -1,0 +1,65 @@
+"""Launch-configuration autotuner of the TMA stencil kernels.
+
+The kernels' results do not depend on the configuration (tile, ring depth,
+occupancy target, z planes per CTA); only their speed does.  For one
+problem the tuner runs short gradient probes (the time loops stopped after
+`nt_probe` steps) on the handle's real grid, model and survey, reads the
+per-kernel CUDA-event timings of the engine, and keeps the fastest forward
+and reverse configurations.
+"""
+from __future__ import annotations
+
+import itertools
+from typing import Dict, Sequence
+
+import torch
+
+FWD_CFGS = (0, 1, 2, 3)
+REV_CFGS = (0, 1, 2, 3)
+ZCHUNKS = (4, 8, 12, 16)
+
+
+def _probe(P, shot_ids, obs, names) -> float:
+    P.profile(1)
+    P.profile_read()
+    P.gradient(shot_ids, obs)
+    torch.cuda.synchronize(P.device)
+    prof = P.profile_read()
+    t = 0.0
+    for n in names:
+        v = prof.get(n, {})
+        if not v.get("timed"):
+            return float("inf")
+        t += v["ms"] / v["timed"]
+    return t
+
+
+def autotune(P, shot_id: int, obs_shot: torch.Tensor, nt_probe: int = 16,
+             fwd_cfgs: Sequence[int] = FWD_CFGS, rev_cfgs: Sequence[int] = REV_CFGS,
+             zchunks: Sequence[int] = ZCHUNKS) -> Dict:
+    """Tunes `P` (a Propagator with model and survey set) on shot `shot_id`
+    whose observed traces are `obs_shot`; returns the timings and the choice."""
+    ids = [int(shot_id)]
+    P.set_nt_limit(nt_probe)
+    try:
+        cur = getattr(P, "tuning", (0, 8, 0, 8))
+        fwd = {}
+        for cfg, zc in itertools.product(fwd_cfgs, zchunks):
+            P.set_tuning(cfg, zc, cur[2], cur[3])
+            _probe(P, ids, obs_shot, ())  # warm (first launch sets attributes)
+            fwd[(cfg, zc)] = _probe(P, ids, obs_shot, ("stress_fwd", "velocity_fwd"))
+        bf = min(fwd, key=fwd.get)
+        rev = {}
+        for cfg, zc in itertools.product(rev_cfgs, zchunks):
+            P.set_tuning(bf[0], bf[1], cfg, zc)
+            _probe(P, ids, obs_shot, ())
+            rev[(cfg, zc)] = _probe(P, ids, obs_shot, ("rev_velocity", "rev_stress"))
+        br = min(rev, key=rev.get)
+    finally:
+        P.set_nt_limit(0)
+        P.profile(0)
+    P.set_tuning(bf[0], bf[1], br[0], br[1])
+    return {"fwd_cfg": bf[0], "zchunk_fwd": bf[1], "rev_cfg": br[0], "zchunk_rev": br[1],
+            "fwd_ms": round(fwd[bf], 4), "rev_ms": round(rev[br], 4),
+            "fwd_default_ms": round(fwd.get((0, 8), float("nan")), 4),
+            "rev_default_ms": round(rev.get((0, 8), float("nan")), 4), "probes": len(fwd) + len(rev)}

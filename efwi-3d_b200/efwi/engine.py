@@ -67,7 +67,7 @@ class Propagator:
     """Elastic forward/adjoint engine for one grid on one GPU."""
 
     def __init__(self, grid: Grid, device=None, if_win: bool = False, tile_bx: int = 4,
-                 zchunk: int = 16, max_batch: int = 4):
+                 zchunk: int = 8, max_batch: int = 4):
         if not torch.cuda.is_available():
             raise RuntimeError("efwi: a CUDA device is required (there is no CPU path)")
         self.grid = grid
@@ -107,6 +107,20 @@ class Propagator:
         self.if_win = bool(if_win)
         check(self._h, self._L.efwi_set_options(self._h, int(if_win), int(tile_bx), int(zchunk),
                                                 int(max_batch)))
+
+    def set_variant(self, variant: int) -> None:
+        """1: TMA-staged stencil planes (default); 0: L1-served stencils."""
+        check(self._h, self._L.efwi_set_variant(self._h, int(variant)))
+
+    def set_tuning(self, fwd_cfg: int = 0, zchunk_fwd: int = 0, rev_cfg: int = 0,
+                   zchunk_rev: int = 0) -> None:
+        """Launch configuration of the TMA kernels (see efwi_set_tuning)."""
+        check(self._h, self._L.efwi_set_tuning(self._h, int(fwd_cfg), int(zchunk_fwd),
+                                               int(rev_cfg), int(zchunk_rev)))
+        self.tuning = (fwd_cfg, zchunk_fwd, rev_cfg, zchunk_rev)
+
+    def set_nt_limit(self, nt_limit: int) -> None:
+        check(self._h, self._L.efwi_set_nt_limit(self._h, int(nt_limit)))
 
     def set_model(self, lam, mu, rho) -> None:
         """lambda, mu, rho on the padded grid, [nz][nx][ny] (any device)."""

@@ -68,6 +68,23 @@ const char *efwi_version(void);
  * per CTA; 0 keeps), max_batch >= 1 shots per forward launch (0 keeps). */
 int efwi_set_options(EfwiHandle *h, int if_win, int tile_bx, int zchunk, int max_batch);
 
+/* Kernel family of the stencil sweeps: 1 (default) stages the x/y-halo
+ * operands of every z plane in shared memory with bulk tensor copies
+ * (TMA); 0 reads them through L1.  Both give identical results.  No
+ * reference counterpart (the reference has one plain kernel per update). */
+int efwi_set_variant(EfwiHandle *h, int variant);
+
+/* Launch configuration of the TMA kernels (the autotuner's knobs; results
+ * do not depend on them): fwd_cfg / rev_cfg in 0..3 select tile, ring depth
+ * and occupancy target; zchunk_* > 0 sets the z planes per CTA (0 keeps).
+ * No reference counterpart. */
+int efwi_set_tuning(EfwiHandle *h, int fwd_cfg, int zchunk_fwd, int rev_cfg, int zchunk_rev);
+
+/* Timing probes: nt_limit > 0 stops the time loops after nt_limit steps
+ * (results are then not meaningful); 0 restores the full axis.  No
+ * reference counterpart. */
+int efwi_set_nt_limit(EfwiHandle *h, int nt_limit);
+
 /* Replaces: Model (Model.cu:15-80) and the CFL check compCourantNumber
  * (utilities.cu:186-202).  lam, mu, rho: device [nz][nx][ny]; copied. */
 int efwi_set_model(EfwiHandle *h, const float *lam, const float *mu, const float *rho,

@@ -165,3 +165,58 @@ def test_bad_shot_id_and_call_order_raise():
     P.set_survey(shots, stf)
     with pytest.raises(EfwiError, match="out of range"):
         P.forward([3])
+
+
+@pytest.mark.parametrize("bx,zchunk", [(4, 16), (8, 5), (8, 64)])
+def test_tma_variant_matches_l1_variant(bx, zchunk):
+    """Stencil planes staged by bulk tensor copies against the L1-served
+    kernels: forward traces and the misfit are bitwise identical; the fused
+    reverse kernels contract a few multiply-adds differently, so their
+    gradients agree to 1e-6 (rel-L2)."""
+    d = golden()
+    a = _prop("A_", tile_bx=bx, zchunk=zchunk, max_batch=2)
+    b = _prop("A_", tile_bx=bx, zchunk=zchunk, max_batch=2)
+    a.set_variant(0)
+    b.set_variant(1)
+    assert torch.equal(a.forward([0, 1]).cpu(), b.forward([0, 1]).cpu())
+    a = _prop("B_", tile_bx=bx, zchunk=zchunk)
+    b = _prop("B_", tile_bx=bx, zchunk=zchunk)
+    a.set_variant(0)
+    b.set_variant(1)
+    obs = torch.from_numpy(d["B_obs"])
+    ra, rb = a.gradient([0], obs), b.gradient([0], obs)
+    assert ra[0] == rb[0]
+    for x, y in zip(ra[1:], rb[1:]):
+        assert rel_l2(y.cpu(), x.cpu()) < 1e-6
+
+
+def test_all_launch_configurations_give_identical_results():
+    """The autotuner's knobs (tile, ring depth, occupancy target, z planes
+    per CTA) change speed only."""
+    d = golden()
+    obs = torch.from_numpy(d["B_obs"])
+    base = _prop("B_")
+    base.set_tuning(0, 8, 0, 8)
+    ref_tr = base.forward([0]).cpu()
+    ref_g = base.gradient([0], obs)
+    for fc, zf, rc, zr in [(1, 4, 1, 4), (2, 12, 2, 16), (3, 5, 3, 3), (0, 64, 1, 64)]:
+        P = _prop("B_")
+        P.set_tuning(fc, zf, rc, zr)
+        assert torch.equal(P.forward([0]).cpu(), ref_tr)
+        g = P.gradient([0], obs)
+        assert g[0] == ref_g[0]
+        for x, y in zip(g[1:], ref_g[1:]):
+            assert torch.equal(x, y)
+
+
+def test_autotuner_keeps_results_and_picks_a_configuration():
+    from efwi.autotune import autotune
+    d = golden()
+    obs = torch.from_numpy(d["B_obs"])
+    P = _prop("B_")
+    before = P.gradient([0], obs)
+    choice = autotune(P, 0, obs, nt_probe=8, zchunks=(4, 8))
+    assert {"fwd_cfg", "rev_cfg", "zchunk_fwd", "zchunk_rev"} <= set(choice)
+    after = P.gradient([0], obs)
+    for x, y in zip(before[1:], after[1:]):
+        assert torch.equal(x, y)
