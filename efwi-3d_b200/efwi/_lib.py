@@ -18,6 +18,8 @@ EFWI_ERR_CUDA = 2
 EFWI_ERR_CFL = 3
 EFWI_ERR_STATE = 4
 EFWI_ERR_NOMEM = 5
+EFWI_ERR_TOO_LARGE = 6
+NOALLOC_MAX_PARTIALS = 65536
 
 MODE_REFERENCE = 0
 MODE_EXACT = 1
@@ -70,6 +72,9 @@ _SIGS = {
     "efwi_gradient": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_int,
                                 C.POINTER(C.c_double), C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p]),
+    "efwi_misfit_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "efwi_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong),
                                     C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

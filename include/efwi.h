@@ -31,6 +31,7 @@ extern "C" {
 #define EFWI_ERR_CFL 3     /* Courant number > 1 (utilities.cu:186-202) */
 #define EFWI_ERR_STATE 4   /* call order: model or survey missing */
 #define EFWI_ERR_NOMEM 5   /* device allocation failed */
+#define EFWI_ERR_TOO_LARGE 6 /* request exceeds a fixed-size buffer (efwi_misfit_noalloc) */
 
 #define EFWI_MODE_REFERENCE 0 /* the reference's gradient (libCUFD.cu:469-613) */
 #define EFWI_MODE_EXACT 1     /* exact discrete adjoint of the forward scheme */
@@ -111,6 +112,26 @@ int efwi_misfit(EfwiHandle *h, int n, const int *shot_ids, const float *obs, dou
 int efwi_gradient(EfwiHandle *h, int n, const int *shot_ids, const float *obs, int mode,
                   double *misfit, float *g_lam, float *g_mu, float *g_rho, float *res,
                   void *stream);
+
+/* Misfit and adjoint source of one shot with no device allocation.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (device memory reserved up front by another allocator, or a
+ * latency-critical path that cannot take cudaMalloc's device-wide
+ * synchronisation); needs no handle.  obs, syn (inputs) and res (output) are
+ * device [3][nrec][nt] traces of one shot; misfit is a device double
+ * (output).  Windowed mode (if_win) takes device [nrec] win_start, win_end
+ * (seconds) and weights; otherwise they may be NULL.  Same window, residual
+ * and sum of squares as efwi_misfit / efwi_gradient.  Scratch: a file-scope
+ * device array of EFWI_NOALLOC_MAX_PARTIALS doubles (512 KiB per GPU, held
+ * until exit); requests needing more than that many 32 x 32 tiles
+ * (3 * ceil(nt/32) * ceil(nrec/32)) return EFWI_ERR_TOO_LARGE.  The first
+ * call on a device looks up the array's address and should come before any
+ * stream capture.  Calls that overlap on the GPU race on the array. */
+#define EFWI_NOALLOC_MAX_PARTIALS 65536
+int efwi_misfit_noalloc(int nrec, int nt, float dt, int if_win, const float *win_start,
+                        const float *win_end, const float *weights, float src_weight,
+                        const float *obs, const float *syn, float *res, double *misfit,
+                        void *stream);
 
 /* Per-kernel timing with CUDA events on the call's stream (every
  * `sample`-th time step; 0 disables).  efwi_profile_read fills, for each
