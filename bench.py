@@ -49,6 +49,11 @@ def parse():
     ap.add_argument("--tile-bx", type=int, default=4)
     ap.add_argument("--zchunk", type=int, default=8)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
+    ap.add_argument("--case", default=None,
+                    help="profiling case 'gradient': one shot of the grid, --nt steps, "
+                         "tuning --tuning, forward of the true model then one gradient")
+    ap.add_argument("--tuning", default="1,4,1,4",
+                    help="forward cfg, forward zchunk, reverse cfg, reverse zchunk")
     return ap.parse_args()
 
 
@@ -236,8 +241,28 @@ def write_dropin_files(tmpdir, prob, obs_split, shot_ids):
     return para
 
 
+def run_case(a):
+    """Small fixed workload for profilers (no timing, no JSON)."""
+    import torch
+    from efwi import synthetic
+    from efwi.engine import Propagator
+    p = synthetic.config2(nt=a.nt, nshot=1, n=a.n)
+    P = Propagator(p.grid)
+    P.set_tuning(*[int(v) for v in a.tuning.split(",")])
+    P.set_survey(p.shots, p.stf)
+    P.set_model(*[torch.from_numpy(x) for x in p.params("true")])
+    obs = P.forward([0])
+    P.set_model(*[torch.from_numpy(x) for x in p.params("init")])
+    J = P.gradient([0], obs)[0]
+    torch.cuda.synchronize()
+    print(f"case {a.case}: grid {p.grid.nz}^3, nt {a.nt}, misfit {J:.6e}")
+
+
 def main():
     a = parse()
+    if a.case:
+        run_case(a)
+        return
     if a.impl == "reference":
         run_reference(a)
         return
