@@ -7,7 +7,9 @@
 //     the survey on every call, libCUFD.cu:52-205);
 //   - forward-only calls advance up to `max_batch` shots per launch;
 //   - the reference gradient runs shot by shot with the boundary shell
-//     stored in HBM, and accumulates the images in shot order.
+//     stored in HBM, and accumulates the images in shot order;
+//   - the exact gradient runs shot by shot with binomial checkpoints of the
+//     whole state in HBM under a byte budget (efwi_revolve.h).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -22,7 +24,9 @@
 #include <vector>
 
 #include "../../include/efwi.h"
+#include "efwi_exact.h"
 #include "efwi_kernels.h"
+#include "efwi_revolve.h"
 
 using namespace efwi;
 
@@ -38,12 +42,16 @@ enum KClass {
   K_SHELL_SAVE,
   K_SHELL_RESTORE,
   K_MISFIT,
+  K_ADJ_STRESS,
+  K_ADJ_VELOCITY,
+  K_CHECKPOINT,
   K_OTHER,
   K_NCLASS
 };
 const char *kKernelNames[K_NCLASS] = {"stress_fwd", "velocity_fwd", "rev_velocity", "rev_stress",
                                       "record", "inject", "shell_save", "shell_restore",
-                                      "misfit", "other"};
+                                      "misfit", "adj_stress", "adj_velocity", "checkpoint",
+                                      "other"};
 
 struct DevBuf {
   void *p = nullptr;
@@ -98,6 +106,12 @@ struct EfwiHandle {
 
   DevBuf fields, psi, adj, traces_tm, res_tm, shell, partial, jdev, recbuf, winbuf, scalar, grad;
   DevBuf status;  // pipeline status word (EFWI_STATUS_*)
+
+  // exact gradient: checkpoint slots and the two adjoint memory-variable sets
+  DevBuf ckpt, apsi;
+  long long ck_budget = 4LL << 30;  // bytes of checkpoint slots
+  long long ck_forward_steps = 0;   // forward steps of the last exact gradient
+  int ck_slots = 0;                 // slots it used
 
   int prof_sample = 0;
   std::vector<cudaEvent_t> ev_pool;
@@ -425,26 +439,49 @@ int forward_step(EfwiHandle *h, Fields f, Psi ps, int S, const SrcArgs &src, con
   return check_launch(h, "forward step");
 }
 
-// Forward of a batch of S shots (ids) into traces_tm (time-major, zeroed
-// here).  When `shell` is set (S must be 1) the boundary shell is stored
-// before every step.
-int run_forward_batch(EfwiHandle *h, const int *ids, int S, float *traces_tm, long long ntr,
-                      RecArgs *rec_out, float *shell, cudaStream_t st) {
+// Tensor maps of the forward kernels over the batch volumes f.
+int make_fwd_maps(EfwiHandle *h, const Fields &f, int S, FwdMaps *maps) {
+  const float *sm[11] = {f.vz, f.vx, f.vy, f.szz, f.sxx, f.syy, f.sxz, f.sxy, f.syz,
+                         h->lam.as<float>(), h->mu.as<float>()};
+  const float *vm[9] = {f.sxz, f.syz, f.sxx, f.sxy, f.syy, f.vz, f.vx, f.vy, h->buoy.as<float>()};
+  const int bxf = fwd_tma_tile(h->fcfg);
+  for (int k = 0; k < 11; ++k) {
+    int rc = make_map(h, &maps->s.m[k], sm[k], k < 9 ? S : 1, k < 3, bxf);
+    if (rc) return rc;
+  }
+  for (int k = 0; k < 9; ++k) {
+    int rc = make_map(h, &maps->v.m[k], vm[k], k < 8 ? S : 1, k < 5, bxf);
+    if (rc) return rc;
+  }
+  return EFWI_OK;
+}
+
+// Zeroed state, receivers, source rows and tensor maps of a batch of S
+// shots (ids) whose traces go to traces_tm (time-major, zeroed here).
+struct Batch {
+  Fields f;
+  Psi ps;
+  RecArgs rec;
+  SrcArgs src;
+  FwdMaps maps;
+  const FwdMaps *mp = nullptr;
+};
+
+int prepare_batch(EfwiHandle *h, const int *ids, int S, float *traces_tm, long long ntr,
+                  cudaStream_t st, Batch *b) {
   const long long N = h->N;
   CK_CUDA(h, h->fields.ensure(sizeof(float) * 9 * N * S));
   CK_CUDA(h, h->psi.ensure(sizeof(float) * psi_per_shot(h->geo) * S));
   CK_CUDA(h, cudaMemsetAsync(h->fields.p, 0, sizeof(float) * 9 * N * S, st));
   CK_CUDA(h, cudaMemsetAsync(h->psi.p, 0, sizeof(float) * psi_per_shot(h->geo) * S, st));
   CK_CUDA(h, cudaMemsetAsync(traces_tm, 0, sizeof(float) * ntr, st));
-  Fields f = fields_at(h->fields.as<float>(), N, S);
-  Psi ps = psi_at(h->psi.as<float>(), h->geo, S);
+  b->f = fields_at(h->fields.as<float>(), N, S);
+  b->ps = psi_at(h->psi.as<float>(), h->geo, S);
 
   long long tot;
   RecHost rh = group_receivers(h, ids, S, &tot);
-  RecArgs rec;
-  int rc = upload_receivers(h, rh, st, &rec);
+  int rc = upload_receivers(h, rh, st, &b->rec);
   if (rc) return rc;
-  if (rec_out) *rec_out = rec;
 
   // per-batch source arrays: cells and tapered stf rows, staged in scalar buf
   const int nt = h->grid.nt;
@@ -457,34 +494,35 @@ int run_forward_batch(EfwiHandle *h, const int *ids, int S, float *traces_tm, lo
   for (int s = 0; s < S; ++s)
     CK_CUDA(h, cudaMemcpyAsync(dstf + (size_t)s * nt, h->stf.as<float>() + (size_t)ids[s] * nt,
                                sizeof(float) * nt, cudaMemcpyDeviceToDevice, st));
-  SrcArgs src{dcell, dstf, nt, 0};
-  FwdMaps maps;
-  const FwdMaps *mp = nullptr;
+  b->src = SrcArgs{dcell, dstf, nt, 0};
+  b->mp = nullptr;
   if (h->variant == 1) {
-    const float *sm[11] = {f.vz, f.vx, f.vy, f.szz, f.sxx, f.syy, f.sxz, f.sxy, f.syz,
-                           h->lam.as<float>(), h->mu.as<float>()};
-    const float *vm[9] = {f.sxz, f.syz, f.sxx, f.sxy, f.syy, f.vz, f.vx, f.vy, h->buoy.as<float>()};
-    const int bxf = fwd_tma_tile(h->fcfg);
-    for (int k = 0; k < 11; ++k) {
-      rc = make_map(h, &maps.s.m[k], sm[k], k < 9 ? S : 1, k < 3, bxf);
-      if (rc) return rc;
-    }
-    for (int k = 0; k < 9; ++k) {
-      rc = make_map(h, &maps.v.m[k], vm[k], k < 8 ? S : 1, k < 5, bxf);
-      if (rc) return rc;
-    }
-    mp = &maps;
+    rc = make_fwd_maps(h, b->f, S, &b->maps);
+    if (rc) return rc;
+    b->mp = &b->maps;
   }
+  return EFWI_OK;
+}
+
+// Forward of a batch of S shots (ids) into traces_tm (time-major, zeroed
+// here).  When `shell` is set (S must be 1) the boundary shell is stored
+// before every step.
+int run_forward_batch(EfwiHandle *h, const int *ids, int S, float *traces_tm, long long ntr,
+                      RecArgs *rec_out, float *shell, cudaStream_t st) {
+  Batch b;
+  int rc = prepare_batch(h, ids, S, traces_tm, ntr, st, &b);
+  if (rc) return rc;
+  if (rec_out) *rec_out = b.rec;
   const int npts = h->npts;
   const int ntl = nt_eff(h);
   for (int it = 0; it <= ntl - 2; ++it) {
     if (shell) {
       Timer t(h, K_SHELL_SAVE, st, it);
-      k_shell_save<<<(npts + 255) / 256, 256, 0, st>>>(f, h->pts.as<int>(), npts,
+      k_shell_save<<<(npts + 255) / 256, 256, 0, st>>>(b.f, h->pts.as<int>(), npts,
                                                        shell + (size_t)it * 9 * npts);
     }
-    src.it = it;
-    rc = forward_step(h, f, ps, S, src, rec, traces_tm, st, it, mp);
+    b.src.it = it;
+    rc = forward_step(h, b.f, b.ps, S, b.src, b.rec, traces_tm, st, it, b.mp);
     if (rc) return rc;
   }
   return check_launch(h, "forward");
@@ -528,6 +566,141 @@ int misfit_shot(EfwiHandle *h, const ShotHost &sh, const float *obs, const float
     k_reduce_sum<<<1, 256, 0, st>>>(h->partial.as<double>(), nb, jdev);
   }
   return check_launch(h, "misfit");
+}
+
+// Floats of one checkpoint: 9 fields and the memory variables of one shot.
+long long state_floats(const EfwiHandle *h) { return 9 * h->N + psi_per_shot(h->geo); }
+
+// Checkpoint slots the budget allows for a run of `blocks` states
+// (S_0 is the zero state and needs none).
+int checkpoint_slots(const EfwiHandle *h, int blocks) {
+  const long long per = state_floats(h) * (long long)sizeof(float);
+  long long s = per > 0 ? h->ck_budget / per : 0;
+  if (s > blocks - 1) s = blocks - 1;
+  return (int)std::max(s, 0LL);
+}
+
+// Adjoint kernels' arguments over the engine's single-shot buffers.
+ExactArgs exact_args(EfwiHandle *h, const Fields &f, const Psi &ps, const Fields &a, int par,
+                     float *g0, float *g1) {
+  ExactArgs A;
+  A.g = h->geo;
+  A.f = f;
+  A.ps = ps;
+  A.a = a;
+  const long long P = psi_per_shot(h->geo);
+  A.lin = psi_at(h->apsi.as<float>() + par * P, h->geo, 1);
+  A.lout = psi_at(h->apsi.as<float>() + (1 - par) * P, h->geo, 1);
+  A.lam = h->lam.as<float>();
+  A.mu = h->mu.as<float>();
+  A.buoy = h->buoy.as<float>();
+  A.g0 = g0;
+  A.g1 = g1;
+  return A;
+}
+
+// Exact gradient of one shot (EFWI_MODE_EXACT).  Forward states are
+// recomputed from binomial checkpoints (efwi_revolve.h); the first sweep
+// records the traces, then the misfit gives the adjoint source and block k
+// (k = nt-1 .. 0, state S_k current) runs
+//   transpose of stress stage k (+ lambda, mu images)      if k <= nt-2
+//   adjoint source -2 * res at sample k                    if k >= 1
+//   transpose of velocity stage k-1 (+ buoyancy image)     if k >= 1.
+// glam, gmu, gB: pitched image accumulators.
+int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res_out,
+               float *glam, float *gmu, float *gB, cudaStream_t st) {
+  const int nt = h->grid.nt;
+  const int ntl = nt_eff(h);
+  const long long N = h->N;
+  const long long P = psi_per_shot(h->geo);
+  const ShotHost &sh = h->shots[id];
+  const long long ntr = 3LL * sh.nrec * nt;
+  CK_CUDA(h, h->traces_tm.ensure(sizeof(float) * std::max(ntr, 1LL)));
+  CK_CUDA(h, h->res_tm.ensure(sizeof(float) * std::max(ntr, 1LL)));
+  CK_CUDA(h, h->adj.ensure(sizeof(float) * 9 * N));
+  CK_CUDA(h, h->apsi.ensure(sizeof(float) * 2 * P));
+
+  const int slots = checkpoint_slots(h, ntl);
+  CkPlan plan;
+  plan.build(ntl, slots, 64LL * ntl + 4096);
+  if (plan.too_long || plan.forward_steps > 16LL * ntl)
+    return fail(h, EFWI_ERR_TOO_LARGE,
+                "checkpoint budget of %lld bytes (%d slots of %lld bytes) is too small for %d steps",
+                h->ck_budget, slots, state_floats(h) * 4, ntl);
+  const long long SF = state_floats(h);
+  CK_CUDA(h, h->ckpt.ensure(sizeof(float) * std::max(1LL, (long long)plan.slots_used * SF)));
+  h->ck_forward_steps = plan.forward_steps;
+  h->ck_slots = plan.slots_used;
+
+  Batch b;
+  int rc = prepare_batch(h, &id, 1, h->traces_tm.as<float>(), ntr, st, &b);
+  if (rc) return rc;
+  Fields a = fields_at(h->adj.as<float>(), N, 1);
+  CK_CUDA(h, cudaMemsetAsync(h->adj.p, 0, sizeof(float) * 9 * N, st));
+  CK_CUDA(h, cudaMemsetAsync(h->apsi.p, 0, sizeof(float) * 2 * P, st));
+  RecArgs norec = b.rec;
+  norec.ncell = 0;
+  float *state = h->fields.as<float>();  // [9N fields][P memory variables]
+  float *psi = h->psi.as<float>();
+  float *ck = h->ckpt.as<float>();
+  int nzc;
+  const int zc = h->zchunk_rev;
+  const dim3 grid = stencil_grid(h, 1, 4, zc, &nzc);
+  int par_s = 0, par_v = 0;
+  bool first = true;
+  for (const CkAction &act : plan.actions) {
+    if (act.op == CK_ADVANCE) {
+      for (int it = act.a; it < act.b; ++it) {
+        b.src.it = it;
+        rc = forward_step(h, b.f, b.ps, 1, b.src, first ? b.rec : norec, h->traces_tm.as<float>(),
+                          st, it, b.mp);
+        if (rc) return rc;
+      }
+    } else if (act.op == CK_STORE) {
+      Timer t(h, K_CHECKPOINT, st, 0);
+      float *dst = ck + (long long)act.a * SF;
+      CK_CUDA(h, cudaMemcpyAsync(dst, state, sizeof(float) * 9 * N, cudaMemcpyDeviceToDevice, st));
+      CK_CUDA(h, cudaMemcpyAsync(dst + 9 * N, psi, sizeof(float) * P, cudaMemcpyDeviceToDevice, st));
+    } else if (act.op == CK_RESTORE) {
+      Timer t(h, K_CHECKPOINT, st, 0);
+      if (act.a < 0) {
+        CK_CUDA(h, cudaMemsetAsync(state, 0, sizeof(float) * 9 * N, st));
+        CK_CUDA(h, cudaMemsetAsync(psi, 0, sizeof(float) * P, st));
+      } else {
+        const float *src = ck + (long long)act.a * SF;
+        CK_CUDA(h, cudaMemcpyAsync(state, src, sizeof(float) * 9 * N, cudaMemcpyDeviceToDevice, st));
+        CK_CUDA(h, cudaMemcpyAsync(psi, src + 9 * N, sizeof(float) * P, cudaMemcpyDeviceToDevice, st));
+      }
+    } else {  // CK_BLOCK
+      const int k = act.a;
+      if (first) {
+        first = false;
+        rc = misfit_shot(h, sh, obs, h->traces_tm.as<float>(), h->res_tm.as<float>(), jdev, st);
+        if (rc) return rc;
+        if (res_out && sh.nrec > 0) {
+          k_traces_to_cr_t<<<dim3((nt + 31) / 32, (sh.nrec + 31) / 32, 3), dim3(32, 8), 0, st>>>(
+              h->res_tm.as<float>(), res_out, nt, sh.nrec);
+          h->launches[K_OTHER]++;
+        }
+      }
+      if (k <= ntl - 2) {
+        Timer t(h, K_ADJ_STRESS, st, k);
+        launch_adj_stress_exact(grid, st, exact_args(h, b.f, b.ps, a, par_s, glam, gmu), zc, nzc);
+        par_s ^= 1;
+      }
+      if (k >= 1) {
+        if (b.rec.ncell > 0) {
+          Timer t(h, K_INJECT, st, k);
+          k_inject<<<(b.rec.ncell + 127) / 128, 128, 0, st>>>(a, N, b.rec, h->res_tm.as<float>(), k,
+                                                              -2.0f);
+        }
+        Timer t(h, K_ADJ_VELOCITY, st, k);
+        launch_adj_velocity_exact(grid, st, exact_args(h, b.f, b.ps, a, par_v, gB, nullptr), zc, nzc);
+        par_v ^= 1;
+      }
+    }
+  }
+  return check_launch(h, "exact gradient");
 }
 
 }  // namespace
@@ -775,12 +948,26 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
   CK_CUDA(h, h->jdev.ensure(sizeof(double) * (n + 8)));
   double *jdev = h->jdev.as<double>() + 1;
   if (n > 0) CK_CUDA(h, cudaMemsetAsync(jdev, 0, sizeof(double) * n, st));
-  if (grad) {
-    CK_CUDA(h, h->adj.ensure(sizeof(float) * 9 * N));
+  if (grad) CK_CUDA(h, h->adj.ensure(sizeof(float) * 9 * N));
+  if (grad && mode == EFWI_MODE_REFERENCE)
     CK_CUDA(h, h->shell.ensure(sizeof(float) * 9 * (size_t)std::max(h->npts, 1) * nt));
-  }
   long long obs_off = 0;
-  for (int k = 0; k < n; ++k) {
+  int n_done_exact = 0;
+  if (grad && mode == EFWI_MODE_EXACT) {
+    for (int k = 0; k < n; ++k) {
+      const ShotHost &sh = h->shots[ids[k]];
+      int rc = exact_shot(h, ids[k], obs + obs_off, jdev + k, res_out ? res_out + obs_off : nullptr,
+                          glam, gmu, grho, st);
+      if (rc) return rc;
+      obs_off += 3LL * sh.nrec * nt;
+    }
+    // grho holds the buoyancy image until here
+    const EfwiGrid &G = h->grid;
+    k_buoy_to_rho<<<1184, 256, 0, st>>>(grho, h->buoy.as<float>(), grho, G.nz, G.nx, G.ny, h->py);
+    h->launches[K_OTHER]++;
+    n_done_exact = n;
+  }
+  for (int k = n_done_exact; k < n; ++k) {
     const ShotHost &sh = h->shots[ids[k]];
     const long long ntr = 3LL * sh.nrec * nt;
     CK_CUDA(h, h->traces_tm.ensure(sizeof(float) * std::max(ntr, 1LL)));
@@ -856,7 +1043,7 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     auto inject = [&](int it) {
       if (rec.ncell == 0) return;
       Timer t(h, K_INJECT, st, it);
-      k_inject<<<(rec.ncell + 127) / 128, 128, 0, st>>>(a, N, rec, h->res_tm.as<float>(), it);
+      k_inject<<<(rec.ncell + 127) / 128, 128, 0, st>>>(a, N, rec, h->res_tm.as<float>(), it, 1.0f);
     };
     auto restore = [&](int it, int stress) {
       if (npts == 0) return;
@@ -915,8 +1102,91 @@ int efwi_gradient(EfwiHandle *h, int n, const int *ids, const float *obs, int mo
   if (rc) return rc;
   if (n > 0 && !obs) return fail(h, EFWI_ERR_ARG, "null obs");
   if (!glam || !gmu || !grho) return fail(h, EFWI_ERR_ARG, "null gradient output");
-  if (mode != EFWI_MODE_REFERENCE) return fail(h, EFWI_ERR_ARG, "gradient mode %d is not available", mode);
+  if (mode != EFWI_MODE_REFERENCE && mode != EFWI_MODE_EXACT)
+    return fail(h, EFWI_ERR_ARG, "gradient mode %d is not available", mode);
   return gradient_impl(h, n, ids, obs, mode, misfit, glam, gmu, grho, res, (cudaStream_t)stream);
+}
+
+int efwi_set_checkpoint_budget(EfwiHandle *h, long long bytes) {
+  if (!h || bytes < 0) return EFWI_ERR_ARG;
+  h->ck_budget = bytes;
+  return EFWI_OK;
+}
+
+long long efwi_state_bytes(const EfwiHandle *h) { return h ? state_floats(h) * 4 : -1; }
+
+int efwi_checkpoint_stats(const EfwiHandle *h, long long *forward_steps, int *slots) {
+  if (!h) return EFWI_ERR_ARG;
+  if (forward_steps) *forward_steps = h->ck_forward_steps;
+  if (slots) *slots = h->ck_slots;
+  return EFWI_OK;
+}
+
+int efwi_checkpoint_plan(int nt, int slots, long long *forward_steps, int *slots_used,
+                         int *repetitions, int *actions, int max_actions) {
+  if (nt < 1 || slots < 0 || max_actions < 0) return -1;
+  CkPlan plan;
+  plan.build(nt, slots, actions ? max_actions : 64LL * nt + 4096);
+  if (plan.too_long) return -1;
+  if (forward_steps) *forward_steps = plan.forward_steps;
+  if (slots_used) *slots_used = plan.slots_used;
+  if (repetitions) *repetitions = plan.repetitions;
+  if (actions)
+    for (size_t k = 0; k < plan.actions.size(); ++k) {
+      actions[3 * k] = plan.actions[k].op;
+      actions[3 * k + 1] = plan.actions[k].a;
+      actions[3 * k + 2] = plan.actions[k].b;
+    }
+  return (int)plan.actions.size();
+}
+
+int efwi_step(EfwiHandle *h, float *state, int transpose, void *stream) {
+  if (!h) return EFWI_ERR_ARG;
+  if (!h->model_set) return fail(h, EFWI_ERR_STATE, "efwi_set_model has not been called");
+  if (!state) return fail(h, EFWI_ERR_ARG, "null state");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long N = h->N, P = psi_per_shot(h->geo);
+  CK_CUDA(h, h->fields.ensure(sizeof(float) * 9 * N));
+  CK_CUDA(h, h->psi.ensure(sizeof(float) * P));
+  CK_CUDA(h, h->adj.ensure(sizeof(float) * 9 * N));
+  CK_CUDA(h, h->apsi.ensure(sizeof(float) * 2 * P));
+  CK_CUDA(h, cudaMemsetAsync(h->fields.p, 0, sizeof(float) * 9 * N, st));
+  CK_CUDA(h, cudaMemsetAsync(h->psi.p, 0, sizeof(float) * P, st));
+  Fields f = fields_at(h->fields.as<float>(), N, 1);
+  Psi ps = psi_at(h->psi.as<float>(), h->geo, 1);
+  int rc = status_reset(h, st);
+  if (rc) return rc;
+  if (!transpose) {
+    k_state_convert<<<1184, 256, 0, st>>>(h->geo, state, f, ps, 1);
+    FwdMaps maps;
+    const FwdMaps *mp = nullptr;
+    if (h->variant == 1) {
+      rc = make_fwd_maps(h, f, 1, &maps);
+      if (rc) return rc;
+      mp = &maps;
+    }
+    RecArgs norec{};
+    SrcArgs nosrc{nullptr, nullptr, h->grid.nt, 0};
+    rc = forward_step(h, f, ps, 1, nosrc, norec, nullptr, st, 0, mp);
+    if (rc) return rc;
+    k_state_convert<<<1184, 256, 0, st>>>(h->geo, state, f, ps, 0);
+  } else {
+    Fields a = fields_at(h->adj.as<float>(), N, 1);
+    Psi ap = psi_at(h->apsi.as<float>(), h->geo, 1);
+    CK_CUDA(h, cudaMemsetAsync(h->adj.p, 0, sizeof(float) * 9 * N, st));
+    CK_CUDA(h, cudaMemsetAsync(h->apsi.p, 0, sizeof(float) * 2 * P, st));
+    k_state_convert<<<1184, 256, 0, st>>>(h->geo, state, a, ap, 1);
+    int nzc;
+    const dim3 grid = stencil_grid(h, 1, 4, h->zchunk_rev, &nzc);
+    launch_adj_velocity_exact(grid, st, exact_args(h, f, ps, a, 0, nullptr, nullptr), h->zchunk_rev, nzc);
+    launch_adj_stress_exact(grid, st, exact_args(h, f, ps, a, 0, nullptr, nullptr), h->zchunk_rev, nzc);
+    Psi out = psi_at(h->apsi.as<float>() + P, h->geo, 1);
+    k_state_convert<<<1184, 256, 0, st>>>(h->geo, state, a, out, 0);
+  }
+  h->launches[K_OTHER] += 2;
+  rc = check_launch(h, "step");
+  if (rc) return rc;
+  return status_check(h, st);
 }
 
 int efwi_profile(EfwiHandle *h, int sample) {

@@ -56,10 +56,13 @@ __global__ void k_record(Fields f, long long N, RecArgs rec, float *traces_tm, i
   }
 }
 
-// res_injection (utilities.cu:497-507): adjoint velocity += residual.
-// Receivers sharing a cell are added one after the other in receiver order
-// (the reference's threads race on such a cell).
-__global__ void k_inject(Fields a, long long N, RecArgs rec, const float *res_tm, int it) {
+// res_injection (utilities.cu:497-507): adjoint velocity += scale * residual
+// (scale 1 in the reference algorithm; -2, the derivative of the squared
+// residual, in the exact adjoint).  Receivers sharing a cell are added one
+// after the other in receiver order (the reference's threads race on such a
+// cell).
+__global__ void k_inject(Fields a, long long N, RecArgs rec, const float *res_tm, int it,
+                         float scale) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= rec.ncell) return;
   const int s = rec.ushot[u];
@@ -69,9 +72,9 @@ __global__ void k_inject(Fields a, long long N, RecArgs rec, const float *res_tm
   float vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
   for (int k = rec.uptr[u]; k < rec.uptr[u + 1]; ++k) {
     const int r = rec.rec[k];
-    vx += t[r];
-    vy += t[nr + r];
-    vz += t[2 * nr + r];
+    vx += scale * t[r];
+    vy += scale * t[nr + r];
+    vz += scale * t[2 * nr + r];
   }
   a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
 }

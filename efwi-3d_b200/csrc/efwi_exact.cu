@@ -1,0 +1,498 @@
+// Exact discrete adjoint of the forward time step, with fused imaging.
+//
+// The forward step (stress.cu:36-97 then velocity.cu:35-96, restated in
+// efwi_fwd.cu) is linear in the state (9 fields + 18 C-PML memory
+// variables) for a fixed model.  These kernels apply its transpose, stage by
+// stage, in gather form: each thread owns one cell of the adjoint state and
+// collects what the forward stencils at its neighbours read from it.  This
+// has no reference counterpart; the reference's adjoint kernels
+// (stress_adj.cu, velocity_adj.cu) keep the material coefficients outside
+// the transposed differences and are not this transpose.
+//
+// Notation for one C-PML-modified derivative of the forward step at cell n:
+//   d = D f / h,  psi' = b psi + a d,  d' = d / K + psi'   (slab cells)
+//   d' = d                                                (other cells)
+// The stage adds c * d' to an output field.  With G = c * (adjoint of the
+// output) and L the adjoint of psi' carried back from the later steps, the
+// adjoint of d is
+//   Q = G / K + a (L + G)    (slab),    Q = G    (other cells),
+// and the adjoint of psi before the stage is b (L + G).  The adjoint of the
+// input field f then gathers -D-transposed Q / h: the transpose of D- is
+// -D+, of D+ is -D-, and of the quirk-Q1 difference (velocity.cu:79)
+// c1 Q[j] - (c1 + c2) Q[j+1] + c2 Q[j+2].  Q is zero outside [2, n-3]^3,
+// the cells the forward step updates.
+//
+// K_EV  transpose of the velocity stage (reads the adjoint velocities at
+//       neighbours, updates the adjoint stresses), + buoyancy image
+//       gB += a_v . (dt * modified stress divergence of the forward state)
+// K_ES  transpose of the stress stage (reads the adjoint stresses, lambda
+//       and mu at neighbours, updates the adjoint velocities), + lambda and
+//       mu images from the forward velocities.
+// The adjoint memory variables are read from `lin` and written to `lout`
+// (two buffers used in turn): neighbours read them while the owner updates.
+//
+// Tiling: a CTA owns a 32 (y) x BX (x) column tile and marches a chunk of z
+// planes; neighbour values come through L1.
+#include "efwi_common.cuh"
+#include "efwi_exact.h"
+
+namespace efwi {
+namespace {
+
+__device__ __forceinline__ float qpml(float G, bool slab, float L, float kinv, float a) {
+  return slab ? G * kinv + a * (L + G) : G;
+}
+
+// 4th-order difference operators over four gathered values.
+//   dminus(q[j-2], q[j-1], q[j], q[j+1]),  dplus(q[j-1], q[j], q[j+1], q[j+2])
+// (efwi_common.cuh) and the transpose of the quirk-Q1 difference.
+__device__ __forceinline__ float dq_t(float p0, float p1, float p2) {
+  return EFWI_C1 * p0 - (EFWI_C1 + EFWI_C2) * p1 + EFWI_C2 * p2;
+}
+
+struct Cell {
+  int z, x, y;
+};
+
+// ------------------------------------------------------------ stress stage
+// Adjoint "G" values of the stress stage at cell n.
+struct GS {
+  float ez, ex, ey, xz, xy, yz;
+};
+
+__device__ __forceinline__ GS gs_at(const ExactArgs &A, long long n) {
+  const float l = A.lam[n], u = A.mu[n], l2u = l + 2.0f * u, dt = A.g.dt;
+  const float azz = A.a.szz[n], axx = A.a.sxx[n], ayy = A.a.syy[n];
+  GS r;
+  r.ez = (l2u * azz + l * (axx + ayy)) * dt;
+  r.ex = (l2u * axx + l * (azz + ayy)) * dt;
+  r.ey = (l2u * ayy + l * (azz + axx)) * dt;
+  r.xz = u * A.a.sxz[n] * dt;
+  r.xy = u * A.a.sxy[n] * dt;
+  r.yz = u * A.a.syz[n] * dt;
+  return r;
+}
+
+__device__ __forceinline__ bool inside(const Geo &g, int z, int x, int y) {
+  return z >= 2 && z <= g.nz - 3 && x >= 2 && x <= g.nx - 3 && y >= 2 && y <= g.ny - 3;
+}
+
+// Q of the z-axis terms of the stress stage at (zn, x, y):
+// ez (slot 0, integer points), vx_z (slot 1, half), vy_z (slot 2, half).
+__device__ __forceinline__ void qs_z(const ExactArgs &A, int zn, int x, int y, float &qez,
+                                     float &qvx, float &qvy) {
+  const Geo &g = A.g;
+  if (zn < 2 || zn > g.nz - 3) { qez = qvx = qvy = 0.f; return; }
+  const long long n = cell(g, zn, x, y);
+  const GS G = gs_at(A, n);
+  if (slab_s(zn, g.nz, g.np)) {
+    const long long k = psi_z_idx(g, zn, x, y);
+    const float *c = g.cz;
+    const int nz = g.nz;
+    qez = qpml(G.ez, true, A.lin.z[PSI_VA * g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+    qvx = qpml(G.xz, true, A.lin.z[PSI_VB1 * g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+    qvy = qpml(G.yz, true, A.lin.z[PSI_VB2 * g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+  } else {
+    qez = G.ez; qvx = G.xz; qvy = G.yz;
+  }
+}
+
+// x-axis terms: ex (slot 0, integer), vz_x (slot 1, half), vy_x (slot 2, half).
+__device__ __forceinline__ void qs_x(const ExactArgs &A, int z, int xn, int y, float &qex,
+                                     float &qvz, float &qvy) {
+  const Geo &g = A.g;
+  if (xn < 2 || xn > g.nx - 3) { qex = qvz = qvy = 0.f; return; }
+  const long long n = cell(g, z, xn, y);
+  const GS G = gs_at(A, n);
+  if (slab_s(xn, g.nx, g.np)) {
+    const long long k = psi_x_idx(g, z, xn, y);
+    const float *c = g.cx;
+    const int nx = g.nx;
+    qex = qpml(G.ex, true, A.lin.x[PSI_VA * g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+    qvz = qpml(G.xz, true, A.lin.x[PSI_VB1 * g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+    qvy = qpml(G.xy, true, A.lin.x[PSI_VB2 * g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+  } else {
+    qex = G.ex; qvz = G.xz; qvy = G.xy;
+  }
+}
+
+// y-axis terms: ey (slot 0, integer), vz_y (slot 1, half), vx_y (slot 2, half).
+__device__ __forceinline__ void qs_y(const ExactArgs &A, int z, int x, int yn, float &qey,
+                                     float &qvz, float &qvx) {
+  const Geo &g = A.g;
+  if (yn < 2 || yn > g.ny - 3) { qey = qvz = qvx = 0.f; return; }
+  const long long n = cell(g, z, x, yn);
+  const GS G = gs_at(A, n);
+  if (slab_s(yn, g.ny, g.np)) {
+    const long long k = psi_y_idx(g, z, x, yn);
+    const float *c = g.cy;
+    const int ny = g.ny;
+    qey = qpml(G.ey, true, A.lin.y[PSI_VA * g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qvz = qpml(G.yz, true, A.lin.y[PSI_VB1 * g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+    qvx = qpml(G.xy, true, A.lin.y[PSI_VB2 * g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+  } else {
+    qey = G.ey; qvz = G.yz; qvx = G.xy;
+  }
+}
+
+template <int BX>
+__global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int zchunk, int nzc) {
+  const Geo &g = A.g;
+  const int y = blockIdx.x * 32 + threadIdx.x;
+  const int x = blockIdx.y * BX + threadIdx.y;
+  const int z0 = max((int)blockIdx.z * zchunk, 2);
+  const int z1 = min((int)blockIdx.z * zchunk + zchunk, g.nz - 2);
+  (void)nzc;
+  if (x < 2 || x > g.nx - 3 || y < 2 || y > g.ny - 3 || z0 >= z1) return;
+  const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
+  const long long sz = g.sz;
+  const int sx = g.sx;
+  const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
+  const bool xs = slab_s(x, nx, np), ys = slab_s(y, ny, np);
+
+  // z-axis Q values of planes z-2 .. z+2 (index 0 .. 4)
+  float qez[5], qvx[5], qvy[5];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) qs_z(A, z0 - 2 + k, x, y, qez[k], qvx[k], qvy[k]);
+
+  for (int z = z0; z < z1; ++z) {
+    qs_z(A, z + 2, x, y, qez[4], qvx[4], qvy[4]);
+    const long long i = cell(g, z, x, y);
+    const bool zs = slab_s(z, nz, np);
+
+    // ---- x- and y-axis Q values at the neighbours
+    float xex[4], xvz[4], xvy[4];  // x-1 .. x+2 (ex) and x-2 .. x+1 (vz, vy)
+    {
+      float e[5], vz5[5], vy5[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) qs_x(A, z, x - 2 + k, y, e[k], vz5[k], vy5[k]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { xex[k] = e[k + 1]; xvz[k] = vz5[k]; xvy[k] = vy5[k]; }
+    }
+    float yey[4], yvz[4], yvx[4];
+    {
+      float e[5], vz5[5], vx5[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) qs_y(A, z, x, y - 2 + k, e[k], vz5[k], vx5[k]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { yey[k] = e[k + 1]; yvz[k] = vz5[k]; yvx[k] = vx5[k]; }
+    }
+
+    // ---- adjoint velocities
+    const float dvz = -dplus(qez[1], qez[2], qez[3], qez[4]) * idz -
+                      dminus(xvz[0], xvz[1], xvz[2], xvz[3]) * idx -
+                      dminus(yvz[0], yvz[1], yvz[2], yvz[3]) * idy;
+    const float dvx = -dplus(xex[0], xex[1], xex[2], xex[3]) * idx -
+                      dminus(qvx[0], qvx[1], qvx[2], qvx[3]) * idz -
+                      dminus(yvx[0], yvx[1], yvx[2], yvx[3]) * idy;
+    const float dvy = -dplus(yey[0], yey[1], yey[2], yey[3]) * idy -
+                      dminus(xvy[0], xvy[1], xvy[2], xvy[3]) * idx -
+                      dminus(qvy[0], qvy[1], qvy[2], qvy[3]) * idz;
+
+    // ---- images from the forward velocities of the same step
+    const float *vz = A.f.vz, *vx = A.f.vx, *vy = A.f.vy;
+    float ezz = dminus(vz[i - 2 * sz], vz[i - sz], vz[i], vz[i + sz]) * idz;
+    float exx = dminus(vx[i - 2 * sx], vx[i - sx], vx[i], vx[i + sx]) * idx;
+    float eyy = dminus(vy[i - 2], vy[i - 1], vy[i], vy[i + 1]) * idy;
+    float dvx_dz = dplus(vx[i - sz], vx[i], vx[i + sz], vx[i + 2 * sz]) * idz;
+    float dvy_dz = dplus(vy[i - sz], vy[i], vy[i + sz], vy[i + 2 * sz]) * idz;
+    float dvx_dy = dplus(vx[i - 1], vx[i], vx[i + 1], vx[i + 2]) * idy;
+    float dvz_dx = dplus(vz[i - sx], vz[i], vz[i + sx], vz[i + 2 * sx]) * idx;
+    float dvz_dy = dplus(vz[i - 1], vz[i], vz[i + 1], vz[i + 2]) * idy;
+    float dvy_dx = dplus(vy[i - sx], vy[i], vy[i + sx], vy[i + 2 * sx]) * idx;
+    const GS G = gs_at(A, i);
+    if (zs) {
+      const float *c = g.cz;
+      const float Kz = c[CK * nz + z], az = c[CA * nz + z], bz = c[CB * nz + z];
+      const float Kzh = c[CKH * nz + z], azh = c[CAH * nz + z], bzh = c[CBH * nz + z];
+      const long long k = psi_z_idx(g, z, x, y);
+      const float *p = A.ps.z;
+      ezz = ezz * Kz + (bz * p[PSI_VA * g.slab_z + k] + az * ezz);
+      dvx_dz = dvx_dz * Kzh + (bzh * p[PSI_VB1 * g.slab_z + k] + azh * dvx_dz);
+      dvy_dz = dvy_dz * Kzh + (bzh * p[PSI_VB2 * g.slab_z + k] + azh * dvy_dz);
+      A.lout.z[PSI_VA * g.slab_z + k] = bz * (A.lin.z[PSI_VA * g.slab_z + k] + G.ez);
+      A.lout.z[PSI_VB1 * g.slab_z + k] = bzh * (A.lin.z[PSI_VB1 * g.slab_z + k] + G.xz);
+      A.lout.z[PSI_VB2 * g.slab_z + k] = bzh * (A.lin.z[PSI_VB2 * g.slab_z + k] + G.yz);
+    }
+    if (xs) {
+      const float *c = g.cx;
+      const float Kx = c[CK * nx + x], ax = c[CA * nx + x], bx = c[CB * nx + x];
+      const float Kxh = c[CKH * nx + x], axh = c[CAH * nx + x], bxh = c[CBH * nx + x];
+      const long long k = psi_x_idx(g, z, x, y);
+      const float *p = A.ps.x;
+      exx = exx * Kx + (bx * p[PSI_VA * g.slab_x + k] + ax * exx);
+      dvz_dx = dvz_dx * Kxh + (bxh * p[PSI_VB1 * g.slab_x + k] + axh * dvz_dx);
+      dvy_dx = dvy_dx * Kxh + (bxh * p[PSI_VB2 * g.slab_x + k] + axh * dvy_dx);
+      A.lout.x[PSI_VA * g.slab_x + k] = bx * (A.lin.x[PSI_VA * g.slab_x + k] + G.ex);
+      A.lout.x[PSI_VB1 * g.slab_x + k] = bxh * (A.lin.x[PSI_VB1 * g.slab_x + k] + G.xz);
+      A.lout.x[PSI_VB2 * g.slab_x + k] = bxh * (A.lin.x[PSI_VB2 * g.slab_x + k] + G.xy);
+    }
+    if (ys) {
+      const float *c = g.cy;
+      const float Ky = c[CK * ny + y], ay = c[CA * ny + y], by = c[CB * ny + y];
+      const float Kyh = c[CKH * ny + y], ayh = c[CAH * ny + y], byh = c[CBH * ny + y];
+      const long long k = psi_y_idx(g, z, x, y);
+      const float *p = A.ps.y;
+      eyy = eyy * Ky + (by * p[PSI_VA * g.slab_y + k] + ay * eyy);
+      dvz_dy = dvz_dy * Kyh + (byh * p[PSI_VB1 * g.slab_y + k] + ayh * dvz_dy);
+      dvx_dy = dvx_dy * Kyh + (byh * p[PSI_VB2 * g.slab_y + k] + ayh * dvx_dy);
+      A.lout.y[PSI_VA * g.slab_y + k] = by * (A.lin.y[PSI_VA * g.slab_y + k] + G.ey);
+      A.lout.y[PSI_VB1 * g.slab_y + k] = byh * (A.lin.y[PSI_VB1 * g.slab_y + k] + G.yz);
+      A.lout.y[PSI_VB2 * g.slab_y + k] = byh * (A.lin.y[PSI_VB2 * g.slab_y + k] + G.xy);
+    }
+    if (A.g0) {
+      const float azz = A.a.szz[i], axx = A.a.sxx[i], ayy = A.a.syy[i];
+      const float axz = A.a.sxz[i], axy = A.a.sxy[i], ayz = A.a.syz[i];
+      A.g0[i] += (azz + axx + ayy) * (ezz + exx + eyy) * dt;
+      A.g1[i] += (2.0f * (azz * ezz + axx * exx + ayy * eyy) + axz * (dvx_dz + dvz_dx) +
+                  axy * (dvx_dy + dvy_dx) + ayz * (dvy_dz + dvz_dy)) * dt;
+    }
+    A.a.vz[i] += dvz;
+    A.a.vx[i] += dvx;
+    A.a.vy[i] += dvy;
+
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { qez[k] = qez[k + 1]; qvx[k] = qvx[k + 1]; qvy[k] = qvy[k + 1]; }
+  }
+}
+
+// ---------------------------------------------------------- velocity stage
+// G of the velocity stage at cell n: adjoint velocity * buoyancy * dt.
+__device__ __forceinline__ void gv_at(const ExactArgs &A, long long n, float &gz, float &gx,
+                                      float &gy) {
+  const float s = A.buoy[n] * A.g.dt;
+  gz = A.a.vz[n] * s;
+  gx = A.a.vx[n] * s;
+  gy = A.a.vy[n] * s;
+}
+
+// z-axis terms of the velocity stage at (zn, x, y):
+// vz <- szz (slot 3, half), vx <- sxz (slot 4, integer), vy <- syz (slot 5, integer).
+__device__ __forceinline__ void qv_z(const ExactArgs &A, int zn, int x, int y, float &qzz,
+                                     float &qxz, float &qyz) {
+  const Geo &g = A.g;
+  if (zn < 2 || zn > g.nz - 3) { qzz = qxz = qyz = 0.f; return; }
+  float gz, gx, gy;
+  gv_at(A, cell(g, zn, x, y), gz, gx, gy);
+  if (slab_s(zn, g.nz, g.np)) {
+    const long long k = psi_z_idx(g, zn, x, y);
+    const float *c = g.cz;
+    const int nz = g.nz;
+    qzz = qpml(gz, true, A.lin.z[PSI_SAA * g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+    qxz = qpml(gx, true, A.lin.z[PSI_SAB1 * g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+    qyz = qpml(gy, true, A.lin.z[PSI_SAB2 * g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+  } else {
+    qzz = gz; qxz = gx; qyz = gy;
+  }
+}
+
+// x-axis terms (quirk-Q2 slabs): vz <- sxz (slot 4, integer), vx <- sxx
+// (slot 3, half), vy <- sxy (slot 5, integer).
+__device__ __forceinline__ void qv_x(const ExactArgs &A, int z, int xn, int y, float &qxz,
+                                     float &qxx, float &qxy) {
+  const Geo &g = A.g;
+  if (xn < 2 || xn > g.nx - 3) { qxz = qxx = qxy = 0.f; return; }
+  float gz, gx, gy;
+  gv_at(A, cell(g, z, xn, y), gz, gx, gy);
+  if (slab_v(xn, g.nx, g.np)) {
+    const long long k = psi_x_idx(g, z, xn, y);
+    const float *c = g.cx;
+    const int nx = g.nx;
+    qxz = qpml(gz, true, A.lin.x[PSI_SAB1 * g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+    qxx = qpml(gx, true, A.lin.x[PSI_SAA * g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+    qxy = qpml(gy, true, A.lin.x[PSI_SAB2 * g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+  } else {
+    qxz = gz; qxx = gx; qxy = gy;
+  }
+}
+
+// y-axis terms (quirk-Q2 slabs): vz <- syz (slot 4, integer), vx <- sxy
+// (slot 5, integer), vy <- syy (slot 3, half).
+__device__ __forceinline__ void qv_y(const ExactArgs &A, int z, int x, int yn, float &qyz,
+                                     float &qxy, float &qyy) {
+  const Geo &g = A.g;
+  if (yn < 2 || yn > g.ny - 3) { qyz = qxy = qyy = 0.f; return; }
+  float gz, gx, gy;
+  gv_at(A, cell(g, z, x, yn), gz, gx, gy);
+  if (slab_v(yn, g.ny, g.np)) {
+    const long long k = psi_y_idx(g, z, x, yn);
+    const float *c = g.cy;
+    const int ny = g.ny;
+    qyz = qpml(gz, true, A.lin.y[PSI_SAB1 * g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qxy = qpml(gx, true, A.lin.y[PSI_SAB2 * g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qyy = qpml(gy, true, A.lin.y[PSI_SAA * g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+  } else {
+    qyz = gz; qxy = gx; qyy = gy;
+  }
+}
+
+template <int BX>
+__global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int zchunk, int nzc) {
+  const Geo &g = A.g;
+  const int y = blockIdx.x * 32 + threadIdx.x;
+  const int x = blockIdx.y * BX + threadIdx.y;
+  const int z0 = max((int)blockIdx.z * zchunk, 2);
+  const int z1 = min((int)blockIdx.z * zchunk + zchunk, g.nz - 2);
+  (void)nzc;
+  if (x < 2 || x > g.nx - 3 || y < 2 || y > g.ny - 3 || z0 >= z1) return;
+  const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
+  const long long sz = g.sz;
+  const int sx = g.sx;
+  const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
+  const bool xs = slab_v(x, nx, np), ys = slab_v(y, ny, np);
+
+  // z-axis Q values of planes z-2 .. z+2
+  float qzz[5], qxz[5], qyz[5];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) qv_z(A, z0 - 2 + k, x, y, qzz[k], qxz[k], qyz[k]);
+
+  for (int z = z0; z < z1; ++z) {
+    qv_z(A, z + 2, x, y, qzz[4], qxz[4], qyz[4]);
+    const long long i = cell(g, z, x, y);
+    const bool zs = slab_s(z, nz, np);
+
+    float x_xz[5], x_xx[5], x_xy[5];  // x-2 .. x+2
+#pragma unroll
+    for (int k = 0; k < 5; ++k) qv_x(A, z, x - 2 + k, y, x_xz[k], x_xx[k], x_xy[k]);
+    float y_yz[5], y_xy[5], y_yy[5];  // y-2 .. y+2
+#pragma unroll
+    for (int k = 0; k < 5; ++k) qv_y(A, z, x, y - 2 + k, y_yz[k], y_xy[k], y_yy[k]);
+
+    // ---- adjoint stresses
+    const float dszz = -dminus(qzz[0], qzz[1], qzz[2], qzz[3]) * idz;
+    const float dsxx = -dminus(x_xx[0], x_xx[1], x_xx[2], x_xx[3]) * idx;
+    const float dsyy = -dminus(y_yy[0], y_yy[1], y_yy[2], y_yy[3]) * idy;
+    const float dsxz = -dplus(x_xz[1], x_xz[2], x_xz[3], x_xz[4]) * idx -
+                       dplus(qxz[1], qxz[2], qxz[3], qxz[4]) * idz;
+    const float dsyz = -dplus(y_yz[1], y_yz[2], y_yz[3], y_yz[4]) * idy -
+                       dplus(qyz[1], qyz[2], qyz[3], qyz[4]) * idz;
+    const float dsxy = -dplus(y_xy[1], y_xy[2], y_xy[3], y_xy[4]) * idy +
+                       dq_t(x_xy[2], x_xy[3], x_xy[4]) * idx;
+
+    // ---- buoyancy image from the forward stresses of the same step
+    const float *szz = A.f.szz, *sxx = A.f.sxx, *syy = A.f.syy;
+    const float *sxz = A.f.sxz, *sxy = A.f.sxy, *syz = A.f.syz;
+    float dszz_dz = dplus(szz[i - sz], szz[i], szz[i + sz], szz[i + 2 * sz]) * idz;
+    float dsxz_dx = dminus(sxz[i - 2 * sx], sxz[i - sx], sxz[i], sxz[i + sx]) * idx;
+    float dsyz_dy = dminus(syz[i - 2], syz[i - 1], syz[i], syz[i + 1]) * idy;
+    float dsxz_dz = dminus(sxz[i - 2 * sz], sxz[i - sz], sxz[i], sxz[i + sz]) * idz;
+    float dsxx_dx = dplus(sxx[i - sx], sxx[i], sxx[i + sx], sxx[i + 2 * sx]) * idx;
+    float dsxy_dy = dminus(sxy[i - 2], sxy[i - 1], sxy[i], sxy[i + 1]) * idy;
+    float dsyz_dz = dminus(syz[i - 2 * sz], syz[i - sz], syz[i], syz[i + sz]) * idz;
+    float dsxy_dx = (EFWI_C1 * (sxy[i] - sxy[i - sx]) - EFWI_C2 * (sxy[i - sx] - sxy[i - 2 * sx])) * idx;
+    float dsyy_dy = dplus(syy[i - 1], syy[i], syy[i + 1], syy[i + 2]) * idy;
+    float gz, gx, gy;
+    gv_at(A, i, gz, gx, gy);
+    if (zs) {
+      const float *c = g.cz;
+      const float Kz = c[CK * nz + z], bz = c[CB * nz + z], Kzh = c[CKH * nz + z], bzh = c[CBH * nz + z];
+      const long long k = psi_z_idx(g, z, x, y);
+      const float *p = A.ps.z;
+      dszz_dz = dszz_dz * Kzh + p[PSI_SAA * g.slab_z + k];
+      dsxz_dz = dsxz_dz * Kz + p[PSI_SAB1 * g.slab_z + k];
+      dsyz_dz = dsyz_dz * Kz + p[PSI_SAB2 * g.slab_z + k];
+      A.lout.z[PSI_SAA * g.slab_z + k] = bzh * (A.lin.z[PSI_SAA * g.slab_z + k] + gz);
+      A.lout.z[PSI_SAB1 * g.slab_z + k] = bz * (A.lin.z[PSI_SAB1 * g.slab_z + k] + gx);
+      A.lout.z[PSI_SAB2 * g.slab_z + k] = bz * (A.lin.z[PSI_SAB2 * g.slab_z + k] + gy);
+    }
+    if (xs) {
+      const float *c = g.cx;
+      const float Kx = c[CK * nx + x], bx = c[CB * nx + x], Kxh = c[CKH * nx + x], bxh = c[CBH * nx + x];
+      const long long k = psi_x_idx(g, z, x, y);
+      const float *p = A.ps.x;
+      dsxz_dx = dsxz_dx * Kx + p[PSI_SAB1 * g.slab_x + k];
+      dsxx_dx = dsxx_dx * Kxh + p[PSI_SAA * g.slab_x + k];
+      dsxy_dx = dsxy_dx * Kx + p[PSI_SAB2 * g.slab_x + k];
+      A.lout.x[PSI_SAB1 * g.slab_x + k] = bx * (A.lin.x[PSI_SAB1 * g.slab_x + k] + gz);
+      A.lout.x[PSI_SAA * g.slab_x + k] = bxh * (A.lin.x[PSI_SAA * g.slab_x + k] + gx);
+      A.lout.x[PSI_SAB2 * g.slab_x + k] = bx * (A.lin.x[PSI_SAB2 * g.slab_x + k] + gy);
+    }
+    if (ys) {
+      const float *c = g.cy;
+      const float Ky = c[CK * ny + y], by = c[CB * ny + y], Kyh = c[CKH * ny + y], byh = c[CBH * ny + y];
+      const long long k = psi_y_idx(g, z, x, y);
+      const float *p = A.ps.y;
+      dsyz_dy = dsyz_dy * Ky + p[PSI_SAB1 * g.slab_y + k];
+      dsxy_dy = dsxy_dy * Ky + p[PSI_SAB2 * g.slab_y + k];
+      dsyy_dy = dsyy_dy * Kyh + p[PSI_SAA * g.slab_y + k];
+      A.lout.y[PSI_SAB1 * g.slab_y + k] = by * (A.lin.y[PSI_SAB1 * g.slab_y + k] + gz);
+      A.lout.y[PSI_SAB2 * g.slab_y + k] = by * (A.lin.y[PSI_SAB2 * g.slab_y + k] + gx);
+      A.lout.y[PSI_SAA * g.slab_y + k] = byh * (A.lin.y[PSI_SAA * g.slab_y + k] + gy);
+    }
+    if (A.g0) {
+      A.g0[i] += (A.a.vz[i] * (dszz_dz + dsxz_dx + dsyz_dy) + A.a.vx[i] * (dsxz_dz + dsxx_dx + dsxy_dy) +
+                  A.a.vy[i] * (dsyz_dz + dsxy_dx + dsyy_dy)) * dt;
+    }
+    A.a.szz[i] += dszz;
+    A.a.sxx[i] += dsxx;
+    A.a.syy[i] += dsyy;
+    A.a.sxz[i] += dsxz;
+    A.a.syz[i] += dsyz;
+    A.a.sxy[i] += dsxy;
+
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { qzz[k] = qzz[k + 1]; qxz[k] = qxz[k + 1]; qyz[k] = qyz[k + 1]; }
+  }
+}
+
+}  // namespace
+
+void launch_adj_stress_exact(dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk, int nzc) {
+  k_adj_stress_exact<4><<<grid, dim3(32, 4), 0, st>>>(A, zchunk, nzc);
+}
+
+void launch_adj_velocity_exact(dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk, int nzc) {
+  k_adj_velocity_exact<4><<<grid, dim3(32, 4), 0, st>>>(A, zchunk, nzc);
+}
+
+// rho image from the buoyancy image: B = 1/rho on [2, n-3]^3
+// (Model.cu:65-76), so dJ/drho = -dJ/dB * B^2 there and 0 elsewhere.
+__global__ void k_buoy_to_rho(const float *gB, const float *buoy, float *grho, int nz, int nx,
+                              int ny, int py) {
+  const long long n = (long long)nz * nx * py;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % py);
+    const long long zx = i / py;
+    const int x = (int)(zx % nx), z = (int)(zx / nx);
+    const bool in = z >= 2 && z <= nz - 3 && x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3;
+    const float b = buoy[i];
+    grho[i] = in ? -gB[i] * b * b : 0.0f;
+  }
+}
+
+// State of the oracle's layout, [27][nz][nx][ny] (9 fields, then the 18
+// memory variables in the order m_vz_z m_vz_x m_vz_y m_vx_z m_vx_x m_vx_y
+// m_vy_z m_vy_x m_vy_y m_szz_z m_sxx_x m_syy_y m_sxz_z m_sxz_x m_sxy_x
+// m_sxy_y m_syz_y m_syz_z), to or from the engine's pitched fields and
+// slab memory variables.  Memory variables outside their slab are not
+// stored; `to_engine` = 0 leaves them unchanged in the full-grid array.
+__constant__ signed char c_psi_axis[18] = {0, 1, 2, 0, 1, 2, 0, 1, 2, 0, 1, 2, 0, 1, 1, 2, 2, 0};
+__constant__ signed char c_psi_slot[18] = {0, 1, 1, 1, 0, 2, 2, 2, 0, 3, 3, 3, 4, 4, 5, 5, 4, 5};
+
+__global__ void k_state_convert(Geo g, float *full, Fields f, Psi ps, int to_engine) {
+  const long long nc = (long long)g.nz * g.nx * g.ny;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 27 * nc;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int comp = (int)(t / nc);
+    const long long r = t - comp * nc;
+    const int y = (int)(r % g.ny);
+    const long long zx = r / g.ny;
+    const int x = (int)(zx % g.nx), z = (int)(zx / g.nx);
+    float *dst = nullptr;
+    if (comp < 9) {
+      float *fl[9] = {f.vz, f.vx, f.vy, f.szz, f.sxx, f.syy, f.sxz, f.sxy, f.syz};
+      dst = fl[comp] + cell(g, z, x, y);
+    } else {
+      const int ax = c_psi_axis[comp - 9], slot = c_psi_slot[comp - 9];
+      if (ax == 0 && slab_s(z, g.nz, g.np)) dst = ps.z + slot * g.slab_z + psi_z_idx(g, z, x, y);
+      if (ax == 1 && slab_s(x, g.nx, g.np)) dst = ps.x + slot * g.slab_x + psi_x_idx(g, z, x, y);
+      if (ax == 2 && slab_s(y, g.ny, g.np)) dst = ps.y + slot * g.slab_y + psi_y_idx(g, z, x, y);
+    }
+    if (!dst) continue;
+    if (to_engine) *dst = full[t];
+    else full[t] = *dst;
+  }
+}
+
+}  // namespace efwi

@@ -1,0 +1,27 @@
+// Exact discrete adjoint kernels (efwi_exact.cu).
+#pragma once
+#include "efwi_common.cuh"
+
+namespace efwi {
+
+struct ExactArgs {
+  Geo g;
+  Fields f;        // forward state S_k (read)
+  Psi ps;          // forward memory variables of S_k (read)
+  Fields a;        // adjoint fields (updated in place)
+  Psi lin, lout;   // adjoint memory variables: read from lin, written to lout
+  const float *lam, *mu, *buoy;
+  float *g0, *g1;  // images: stress stage (lambda, mu); velocity stage (buoyancy, unused)
+};
+
+// Transpose of the stress stage of step k (+ lambda/mu images), then of the
+// velocity stage of step k-1 (+ buoyancy image); the grid is
+// (ceil(ny/32), ceil(nx/4), ceil(nz/zchunk)) with 32 x 4 threads.
+void launch_adj_stress_exact(dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk, int nzc);
+void launch_adj_velocity_exact(dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk, int nzc);
+
+__global__ void k_buoy_to_rho(const float *gB, const float *buoy, float *grho, int nz, int nx,
+                              int ny, int py);
+__global__ void k_state_convert(Geo g, float *full, Fields f, Psi ps, int to_engine);
+
+}  // namespace efwi

@@ -80,7 +80,8 @@ __global__ void k_prep_buoyancy(const float *rho, float *buoy, int nz, int nx, i
 __global__ void k_pitch_copy(const float *src, float *dst, int nz, int nx, int ny, int py,
                              int to_pitched);
 __global__ void k_record(Fields f, long long N, RecArgs rec, float *traces_tm, int it);
-__global__ void k_inject(Fields a, long long N, RecArgs rec, const float *res_tm, int it);
+__global__ void k_inject(Fields a, long long N, RecArgs rec, const float *res_tm, int it,
+                         float scale);
 __global__ void k_shell_save(Fields f, const int *pts, int npts, float *dst);
 __global__ void k_shell_restore(Fields f, const int *pts, int npts, const float *src, int stress);
 

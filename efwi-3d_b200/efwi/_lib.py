@@ -75,6 +75,13 @@ _SIGS = {
     "efwi_misfit_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    "efwi_set_checkpoint_budget": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "efwi_state_bytes": (C.c_longlong, [C.c_void_p]),
+    "efwi_checkpoint_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
+    "efwi_checkpoint_plan": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong),
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int), C.c_int]),
+    "efwi_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "efwi_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "efwi_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong),
                                     C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
@@ -118,3 +125,22 @@ def check(handle, rc: int) -> None:
 def kernel_names():
     L = lib()
     return [L.efwi_kernel_name(k).decode() for k in range(L.efwi_kernel_count())]
+
+
+def checkpoint_plan(nt: int, slots: int, with_actions: bool = False) -> dict:
+    """Binomial checkpoint schedule of the exact gradient (host only, no GPU):
+    forward steps, slots used, repetition number and, optionally, the
+    actions as (op, a, b) rows (op 0 advance a->b, 1 store slot a, 2 restore
+    slot a (-1: zero state), 3 adjoint block a)."""
+    L = lib()
+    fs, su, rep = C.c_longlong(0), C.c_int(0), C.c_int(0)
+    n = L.efwi_checkpoint_plan(nt, slots, C.byref(fs), C.byref(su), C.byref(rep), None, 0)
+    if n < 0:
+        raise ValueError(f"no checkpoint schedule for nt={nt}, slots={slots}")
+    out = {"forward_steps": fs.value, "slots_used": su.value, "repetitions": rep.value,
+           "actions": n}
+    if with_actions:
+        buf = (C.c_int * (3 * n))()
+        L.efwi_checkpoint_plan(nt, slots, None, None, None, buf, n)
+        out["actions"] = [tuple(buf[3 * k:3 * k + 3]) for k in range(n)]
+    return out

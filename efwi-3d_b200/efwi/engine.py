@@ -232,6 +232,33 @@ class Propagator:
             return J.value, gl, gm, gr, res
         return J.value, gl, gm, gr
 
+    # ------------------------------------------------- exact-adjoint support
+    def set_checkpoint_budget(self, nbytes: int) -> None:
+        """HBM bytes for the exact gradient's checkpoint slots."""
+        check(self._h, self._L.efwi_set_checkpoint_budget(self._h, int(nbytes)))
+
+    def state_bytes(self) -> int:
+        """Bytes of one checkpointed state (9 fields + C-PML slabs)."""
+        return int(self._L.efwi_state_bytes(self._h))
+
+    def checkpoint_stats(self) -> dict:
+        fs, sl = C.c_longlong(0), C.c_int(0)
+        check(self._h, self._L.efwi_checkpoint_stats(self._h, C.byref(fs), C.byref(sl)))
+        return {"forward_steps": fs.value, "slots": sl.value}
+
+    def step(self, state: torch.Tensor, transpose: bool = False) -> torch.Tensor:
+        """One source-free forward step (or its exact transpose) of a
+        [27, nz, nx, ny] state: 9 fields then 18 C-PML memory variables in
+        the oracle's order.  Returns the new state (a device copy)."""
+        st = _f32_dev(state, self.device).clone()
+        if tuple(st.shape) != (27,) + tuple(self.grid.shape):
+            raise ValueError(f"state shape {tuple(st.shape)} != (27, {self.grid.shape})")
+        with torch.cuda.device(self.device):
+            rc = self._L.efwi_step(self._h, C.c_void_p(st.data_ptr()), int(bool(transpose)),
+                                   self._stream())
+        check(self._h, rc)
+        return st
+
     # ------------------------------------------------------------ profiling
     def profile(self, sample: int) -> None:
         check(self._h, self._L.efwi_profile(self._h, int(sample)))

@@ -108,10 +108,43 @@ int efwi_misfit(EfwiHandle *h, int n, const int *shot_ids, const float *obs, dou
 /* Replaces: cufd with calc_id 1 (misfit and gradients, libCUFD.cu:220-652).
  * g_lam, g_mu, g_rho: device [nz][nx][ny], overwritten.  mode:
  * EFWI_MODE_REFERENCE or EFWI_MODE_EXACT.  res (optional, device, traces
- * layout): receives the adjoint source of each shot. */
+ * layout): receives the adjoint source of each shot.
+ * EFWI_MODE_REFERENCE follows the reference's algorithm (boundary-shell
+ * reconstruction and its adjoint kernels, libCUFD.cu:469-613).
+ * EFWI_MODE_EXACT (no reference counterpart) returns dJ/dlambda, dJ/dmu and
+ * dJ/drho of the returned misfit J, by the exact discrete adjoint of the
+ * forward scheme with binomial checkpointing of the whole state under the
+ * byte budget of efwi_set_checkpoint_budget; it returns EFWI_ERR_TOO_LARGE
+ * when the budget would need more than 16 forward steps per time step. */
 int efwi_gradient(EfwiHandle *h, int n, const int *shot_ids, const float *obs, int mode,
                   double *misfit, float *g_lam, float *g_mu, float *g_rho, float *res,
                   void *stream);
+
+/* Exact-gradient checkpoints (no reference counterpart; the reference keeps
+ * only the boundary shell, Boundary.cu).  bytes: HBM for checkpoint slots
+ * (default 4 GiB); one slot holds one state of efwi_state_bytes(h) bytes.
+ * efwi_checkpoint_stats: forward steps and slots of the last exact
+ * gradient's shot.  efwi_checkpoint_plan (host only, no handle): the
+ * schedule for nt time steps and `slots` slots -- total forward steps,
+ * slots used, repetition number, and (if actions is not NULL) up to
+ * max_actions (op, a, b) triples with op 0 advance a->b, 1 store slot a,
+ * 2 restore slot a (-1: the zero state), 3 adjoint block a.  Returns the
+ * number of actions, or -1 if they exceed max_actions. */
+int efwi_set_checkpoint_budget(EfwiHandle *h, long long bytes);
+long long efwi_state_bytes(const EfwiHandle *h);
+int efwi_checkpoint_stats(const EfwiHandle *h, long long *forward_steps, int *slots);
+int efwi_checkpoint_plan(int nt, int slots, long long *forward_steps, int *slots_used,
+                         int *repetitions, int *actions, int max_actions);
+
+/* One time step of the forward scheme without source (transpose = 0; the
+ * linear map of stress.cu:36-97 then velocity.cu:35-96), or of its exact
+ * transpose (transpose = 1), applied in place to a device state
+ * [27][nz][nx][ny]: vz vx vy szz sxx syy sxz sxy syz, then the memory
+ * variables m_vz_z m_vz_x m_vz_y m_vx_z m_vx_x m_vx_y m_vy_z m_vy_x m_vy_y
+ * m_szz_z m_sxx_x m_syy_y m_sxz_z m_sxz_x m_sxy_x m_sxy_y m_syz_y m_syz_z
+ * (full grids; only their C-PML slabs are read and written).  No reference
+ * counterpart; it serves dot-product tests of the adjoint. */
+int efwi_step(EfwiHandle *h, float *state, int transpose, void *stream);
 
 /* Misfit and adjoint source of one shot with no device allocation.  No
  * counterpart in the reference.  For callers that cannot call cudaMalloc
