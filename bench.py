@@ -49,9 +49,14 @@ def parse():
     ap.add_argument("--tile-bx", type=int, default=4)
     ap.add_argument("--zchunk", type=int, default=8)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
+    ap.add_argument("--mode", default="reference", choices=["reference", "exact"],
+                    help="gradient algorithm: the reference's (headline) or the exact "
+                         "discrete adjoint with binomial checkpoints")
+    ap.add_argument("--ck-budget", type=float, default=16.0,
+                    help="GiB of checkpoint slots of the exact gradient")
     ap.add_argument("--case", default=None,
-                    help="profiling case 'gradient': one shot of the grid, --nt steps, "
-                         "tuning --tuning, forward of the true model then one gradient")
+                    help="profiling case 'gradient' or 'exact': one shot of the grid, --nt "
+                         "steps, tuning --tuning, forward of the true model then one gradient")
     ap.add_argument("--tuning", default="1,4,1,4",
                     help="forward cfg, forward zchunk, reverse cfg, reverse zchunk")
     return ap.parse_args()
@@ -136,11 +141,19 @@ def kernel_bytes(grid, nshot_launch=1):
                   stresses, r/w lambda and mu images; adjoint stress: 3
                   adjoint velocities, lambda, mu, B, r/w 6 adjoint stresses)
                   + 36 B per slab cell
+    adj_stress  : 21 floats per cell (exact transpose of the stress stage:
+                  6 adjoint stresses, lambda, mu, 3 forward velocities, r/w 3
+                  adjoint velocities, r/w lambda and mu images)
+                  + 36 B per slab cell (3 forward psi, 3 adjoint psi in, 3 out)
+    adj_velocity: 24 floats per cell (3 adjoint velocities, B, 6 forward
+                  stresses, r/w 6 adjoint stresses, r/w buoyancy image)
+                  + 36 B per slab cell
     """
     n = grid.ncell
     S = 2 * grid.npml * (grid.nx * grid.ny + grid.nz * grid.ny + grid.nz * grid.nx)
     per = {"stress_fwd": 68 * n + 24 * S, "velocity_fwd": 52 * n + 24 * S,
-           "rev_velocity": 116 * n + 36 * S, "rev_stress": 148 * n + 36 * S}
+           "rev_velocity": 116 * n + 36 * S, "rev_stress": 148 * n + 36 * S,
+           "adj_stress": 84 * n + 36 * S, "adj_velocity": 96 * n + 36 * S}
     return {k: v * nshot_launch for k, v in per.items()}
 
 
@@ -253,7 +266,8 @@ def run_case(a):
     P.set_model(*[torch.from_numpy(x) for x in p.params("true")])
     obs = P.forward([0])
     P.set_model(*[torch.from_numpy(x) for x in p.params("init")])
-    J = P.gradient([0], obs)[0]
+    P.set_checkpoint_budget(int(a.ck_budget * (1 << 30)))
+    J = P.gradient([0], obs, mode="exact" if a.case == "exact" else "reference")[0]
     torch.cuda.synchronize()
     print(f"case {a.case}: grid {p.grid.nz}^3, nt {a.nt}, misfit {J:.6e}")
 
@@ -288,6 +302,7 @@ def main():
     g = prob.grid
     ids = list(range(len(prob.shots)))
     P = Propagator(g, device=dev, tile_bx=a.tile_bx, zchunk=a.zchunk, max_batch=4)
+    P.set_checkpoint_budget(int(a.ck_budget * (1 << 30)))
     P.set_survey(prob.shots, prob.stf)
     lt, mt, rt = prob.params("true")
     P.set_model(torch.from_numpy(lt), torch.from_numpy(mt), torch.from_numpy(rt))
@@ -301,7 +316,7 @@ def main():
     stream = torch.cuda.current_stream(dev)
 
     def step():
-        J, gl, gm, gr = P.gradient(ids, obs)
+        J, gl, gm, gr = P.gradient(ids, obs, mode=a.mode)
         if world > 1:
             jt = torch.tensor([J], device=dev, dtype=torch.float32)
             for t in (gl, gm, gr, jt):
@@ -363,7 +378,7 @@ def main():
 
     # --------------------------------------------------- e2e through fwi_ops
     e2e = None
-    if not a.no_e2e:
+    if not a.no_e2e and a.mode == "reference":
         import FWI_ops_3d as F
         with tempfile.TemporaryDirectory() as tmp:
             para = write_dropin_files(tmp, prob, P.split(obs, ids), ids)
@@ -406,9 +421,10 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"config2: {a.n}^3 model ({g.nz}^3 padded, C-PML {g.npml}),"
-                                       f" {len(ids)} shots per GPU, nt={g.nt}, reference gradient",
+                                       f" {len(ids)} shots per GPU, nt={g.nt}, {a.mode} gradient",
                            "model_cells": a.n, "padded": g.nz, "shots_per_gpu": len(ids),
-                           "nt": g.nt, "mode": "reference",
+                           "nt": g.nt, "mode": a.mode,
+                           "checkpoints": P.checkpoint_stats() if a.mode == "exact" else None,
                            "l2": "inputs larger than L2 (9 fields x 14 MB per shot + shell store)",
                            "autotune": tune},
                 "roofline": roof, "step_roofline": whole, "cpu_baseline": cpu, "e2e": e2e,

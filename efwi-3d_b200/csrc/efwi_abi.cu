@@ -645,7 +645,8 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
   float *ck = h->ckpt.as<float>();
   int nzc;
   const int zc = h->zchunk_rev;
-  const dim3 grid = stencil_grid(h, 1, 4, zc, &nzc);
+  const int bxe = h->bx;
+  const dim3 grid = stencil_grid(h, 1, bxe, zc, &nzc);
   int par_s = 0, par_v = 0;
   bool first = true;
   for (const CkAction &act : plan.actions) {
@@ -685,7 +686,7 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
       }
       if (k <= ntl - 2) {
         Timer t(h, K_ADJ_STRESS, st, k);
-        launch_adj_stress_exact(grid, st, exact_args(h, b.f, b.ps, a, par_s, glam, gmu), zc, nzc);
+        launch_adj_stress_exact(bxe, grid, st, exact_args(h, b.f, b.ps, a, par_s, glam, gmu), zc, nzc);
         par_s ^= 1;
       }
       if (k >= 1) {
@@ -695,7 +696,7 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
                                                               -2.0f);
         }
         Timer t(h, K_ADJ_VELOCITY, st, k);
-        launch_adj_velocity_exact(grid, st, exact_args(h, b.f, b.ps, a, par_v, gB, nullptr), zc, nzc);
+        launch_adj_velocity_exact(bxe, grid, st, exact_args(h, b.f, b.ps, a, par_v, gB, nullptr), zc, nzc);
         par_v ^= 1;
       }
     }
@@ -1177,9 +1178,9 @@ int efwi_step(EfwiHandle *h, float *state, int transpose, void *stream) {
     CK_CUDA(h, cudaMemsetAsync(h->apsi.p, 0, sizeof(float) * 2 * P, st));
     k_state_convert<<<1184, 256, 0, st>>>(h->geo, state, a, ap, 1);
     int nzc;
-    const dim3 grid = stencil_grid(h, 1, 4, h->zchunk_rev, &nzc);
-    launch_adj_velocity_exact(grid, st, exact_args(h, f, ps, a, 0, nullptr, nullptr), h->zchunk_rev, nzc);
-    launch_adj_stress_exact(grid, st, exact_args(h, f, ps, a, 0, nullptr, nullptr), h->zchunk_rev, nzc);
+    const dim3 grid = stencil_grid(h, 1, h->bx, h->zchunk_rev, &nzc);
+    launch_adj_velocity_exact(h->bx, grid, st, exact_args(h, f, ps, a, 0, nullptr, nullptr), h->zchunk_rev, nzc);
+    launch_adj_stress_exact(h->bx, grid, st, exact_args(h, f, ps, a, 0, nullptr, nullptr), h->zchunk_rev, nzc);
     Psi out = psi_at(h->apsi.as<float>() + P, h->geo, 1);
     k_state_convert<<<1184, 256, 0, st>>>(h->geo, state, a, out, 0);
   }

@@ -32,12 +32,28 @@
 // (two buffers used in turn): neighbours read them while the owner updates.
 //
 // Tiling: a CTA owns a 32 (y) x BX (x) column tile and marches a chunk of z
-// planes; neighbour values come through L1.
+// planes.  The Q of the x- and y-axis terms are staged in shared memory per
+// plane (tile plus a 2-cell halo), those of the z-axis terms in register
+// queues; the forward fields of the images are read through L1.
 #include "efwi_common.cuh"
 #include "efwi_exact.h"
 
 namespace efwi {
 namespace {
+
+// 32-bit offsets: a volume holds fewer than 2^31 cells (checked by efwi_create).
+__device__ __forceinline__ int cell32(const Geo &g, int z, int x, int y) {
+  return (z * g.nx + x) * g.sx + y;
+}
+__device__ __forceinline__ int psi32_z(const Geo &g, int z, int x, int y) {
+  return (slab_c(z, g.nz, g.np) * g.nx + x) * g.ny + y;
+}
+__device__ __forceinline__ int psi32_x(const Geo &g, int z, int x, int y) {
+  return (z * (2 * g.np) + slab_c(x, g.nx, g.np)) * g.ny + y;
+}
+__device__ __forceinline__ int psi32_y(const Geo &g, int z, int x, int y) {
+  return (z * g.nx + x) * (2 * g.np) + slab_c(y, g.ny, g.np);
+}
 
 __device__ __forceinline__ float qpml(float G, bool slab, float L, float kinv, float a) {
   return slab ? G * kinv + a * (L + G) : G;
@@ -50,17 +66,13 @@ __device__ __forceinline__ float dq_t(float p0, float p1, float p2) {
   return EFWI_C1 * p0 - (EFWI_C1 + EFWI_C2) * p1 + EFWI_C2 * p2;
 }
 
-struct Cell {
-  int z, x, y;
-};
-
 // ------------------------------------------------------------ stress stage
 // Adjoint "G" values of the stress stage at cell n.
 struct GS {
   float ez, ex, ey, xz, xy, yz;
 };
 
-__device__ __forceinline__ GS gs_at(const ExactArgs &A, long long n) {
+__device__ __forceinline__ GS gs_at(const ExactArgs &A, int n) {
   const float l = A.lam[n], u = A.mu[n], l2u = l + 2.0f * u, dt = A.g.dt;
   const float azz = A.a.szz[n], axx = A.a.sxx[n], ayy = A.a.syy[n];
   GS r;
@@ -73,25 +85,21 @@ __device__ __forceinline__ GS gs_at(const ExactArgs &A, long long n) {
   return r;
 }
 
-__device__ __forceinline__ bool inside(const Geo &g, int z, int x, int y) {
-  return z >= 2 && z <= g.nz - 3 && x >= 2 && x <= g.nx - 3 && y >= 2 && y <= g.ny - 3;
-}
-
 // Q of the z-axis terms of the stress stage at (zn, x, y):
 // ez (slot 0, integer points), vx_z (slot 1, half), vy_z (slot 2, half).
 __device__ __forceinline__ void qs_z(const ExactArgs &A, int zn, int x, int y, float &qez,
                                      float &qvx, float &qvy) {
   const Geo &g = A.g;
   if (zn < 2 || zn > g.nz - 3) { qez = qvx = qvy = 0.f; return; }
-  const long long n = cell(g, zn, x, y);
+  const int n = cell32(g, zn, x, y);
   const GS G = gs_at(A, n);
   if (slab_s(zn, g.nz, g.np)) {
-    const long long k = psi_z_idx(g, zn, x, y);
+    const int k = psi32_z(g, zn, x, y);
     const float *c = g.cz;
     const int nz = g.nz;
-    qez = qpml(G.ez, true, A.lin.z[PSI_VA * g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
-    qvx = qpml(G.xz, true, A.lin.z[PSI_VB1 * g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
-    qvy = qpml(G.yz, true, A.lin.z[PSI_VB2 * g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+    qez = qpml(G.ez, true, A.lin.z[PSI_VA * (int)g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+    qvx = qpml(G.xz, true, A.lin.z[PSI_VB1 * (int)g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+    qvy = qpml(G.yz, true, A.lin.z[PSI_VB2 * (int)g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
   } else {
     qez = G.ez; qvx = G.xz; qvy = G.yz;
   }
@@ -102,15 +110,15 @@ __device__ __forceinline__ void qs_x(const ExactArgs &A, int z, int xn, int y, f
                                      float &qvz, float &qvy) {
   const Geo &g = A.g;
   if (xn < 2 || xn > g.nx - 3) { qex = qvz = qvy = 0.f; return; }
-  const long long n = cell(g, z, xn, y);
+  const int n = cell32(g, z, xn, y);
   const GS G = gs_at(A, n);
   if (slab_s(xn, g.nx, g.np)) {
-    const long long k = psi_x_idx(g, z, xn, y);
+    const int k = psi32_x(g, z, xn, y);
     const float *c = g.cx;
     const int nx = g.nx;
-    qex = qpml(G.ex, true, A.lin.x[PSI_VA * g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
-    qvz = qpml(G.xz, true, A.lin.x[PSI_VB1 * g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
-    qvy = qpml(G.xy, true, A.lin.x[PSI_VB2 * g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+    qex = qpml(G.ex, true, A.lin.x[PSI_VA * (int)g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+    qvz = qpml(G.xz, true, A.lin.x[PSI_VB1 * (int)g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+    qvy = qpml(G.xy, true, A.lin.x[PSI_VB2 * (int)g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
   } else {
     qex = G.ex; qvz = G.xz; qvy = G.xy;
   }
@@ -121,136 +129,184 @@ __device__ __forceinline__ void qs_y(const ExactArgs &A, int z, int x, int yn, f
                                      float &qvz, float &qvx) {
   const Geo &g = A.g;
   if (yn < 2 || yn > g.ny - 3) { qey = qvz = qvx = 0.f; return; }
-  const long long n = cell(g, z, x, yn);
+  const int n = cell32(g, z, x, yn);
   const GS G = gs_at(A, n);
   if (slab_s(yn, g.ny, g.np)) {
-    const long long k = psi_y_idx(g, z, x, yn);
+    const int k = psi32_y(g, z, x, yn);
     const float *c = g.cy;
     const int ny = g.ny;
-    qey = qpml(G.ey, true, A.lin.y[PSI_VA * g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
-    qvz = qpml(G.yz, true, A.lin.y[PSI_VB1 * g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
-    qvx = qpml(G.xy, true, A.lin.y[PSI_VB2 * g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+    qey = qpml(G.ey, true, A.lin.y[PSI_VA * (int)g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qvz = qpml(G.yz, true, A.lin.y[PSI_VB1 * (int)g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+    qvx = qpml(G.xy, true, A.lin.y[PSI_VB2 * (int)g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
   } else {
     qey = G.ey; qvz = G.yz; qvx = G.xy;
   }
 }
 
+// Own cell of the stress stage: G and the Q of its x- and y-axis terms.
+__device__ __forceinline__ GS qs_own(const ExactArgs &A, int z, int x, int y, float qx[3],
+                                     float qy[3]) {
+  const Geo &g = A.g;
+  const GS G = gs_at(A, cell32(g, z, x, y));
+  if (slab_s(x, g.nx, g.np)) {
+    const int k = psi32_x(g, z, x, y);
+    const float *c = g.cx;
+    const int nx = g.nx;
+    qx[0] = qpml(G.ex, true, A.lin.x[PSI_VA * (int)g.slab_x + k], c[CK * nx + x], c[CA * nx + x]);
+    qx[1] = qpml(G.xz, true, A.lin.x[PSI_VB1 * (int)g.slab_x + k], c[CKH * nx + x], c[CAH * nx + x]);
+    qx[2] = qpml(G.xy, true, A.lin.x[PSI_VB2 * (int)g.slab_x + k], c[CKH * nx + x], c[CAH * nx + x]);
+  } else {
+    qx[0] = G.ex; qx[1] = G.xz; qx[2] = G.xy;
+  }
+  if (slab_s(y, g.ny, g.np)) {
+    const int k = psi32_y(g, z, x, y);
+    const float *c = g.cy;
+    const int ny = g.ny;
+    qy[0] = qpml(G.ey, true, A.lin.y[PSI_VA * (int)g.slab_y + k], c[CK * ny + y], c[CA * ny + y]);
+    qy[1] = qpml(G.yz, true, A.lin.y[PSI_VB1 * (int)g.slab_y + k], c[CKH * ny + y], c[CAH * ny + y]);
+    qy[2] = qpml(G.xy, true, A.lin.y[PSI_VB2 * (int)g.slab_y + k], c[CKH * ny + y], c[CAH * ny + y]);
+  } else {
+    qy[0] = G.ey; qy[1] = G.yz; qy[2] = G.xy;
+  }
+  return G;
+}
+
+// Per z plane, the CTA evaluates the Q of the x-axis terms on its tile plus
+// two rows on each side, and of the y-axis terms plus two columns on each
+// side, into shared memory (one evaluation per point); the z-axis terms of
+// the thread's own column run in a register queue of planes z-2 .. z+2.
+// The shared buffers alternate by plane parity, so one barrier per plane
+// separates the writes of a plane from the reads of the plane before.
 template <int BX>
 __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int zchunk, int nzc) {
+  __shared__ float sqx[2][3][BX + 4][32];
+  __shared__ float sqy[2][3][BX][36];
   const Geo &g = A.g;
-  const int y = blockIdx.x * 32 + threadIdx.x;
-  const int x = blockIdx.y * BX + threadIdx.y;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int y = blockIdx.x * 32 + tx;
+  const int x = blockIdx.y * BX + ty;
   const int z0 = max((int)blockIdx.z * zchunk, 2);
   const int z1 = min((int)blockIdx.z * zchunk + zchunk, g.nz - 2);
   (void)nzc;
-  if (x < 2 || x > g.nx - 3 || y < 2 || y > g.ny - 3 || z0 >= z1) return;
+  if (z0 >= z1) return;  // uniform over the CTA
   const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
-  const long long sz = g.sz;
+  const int sz = (int)g.sz;
   const int sx = g.sx;
   const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
+  const bool xin = x >= 2 && x <= nx - 3, yin = y >= 2 && y <= ny - 3;
+  const bool act = xin && yin;
   const bool xs = slab_s(x, nx, np), ys = slab_s(y, ny, np);
+  // halo roles: rows 0, 1, BX+2, BX+3 of sqx (threads ty < 4) and columns
+  // 0, 1, 34, 35 of sqy (threads tx < 4)
+  const int hr = ty < 2 ? ty : BX + ty;
+  const int hxn = (int)blockIdx.y * BX - 2 + hr;
+  const int hc = tx < 2 ? tx : 32 + tx;
+  const int hyn = (int)blockIdx.x * 32 - 2 + hc;
 
-  // z-axis Q values of planes z-2 .. z+2 (index 0 .. 4)
   float qez[5], qvx[5], qvy[5];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) qs_z(A, z0 - 2 + k, x, y, qez[k], qvx[k], qvy[k]);
+  for (int k = 0; k < 4; ++k) {
+    qez[k] = qvx[k] = qvy[k] = 0.f;
+    if (act) qs_z(A, z0 - 2 + k, x, y, qez[k], qvx[k], qvy[k]);
+  }
 
-  for (int z = z0; z < z1; ++z) {
-    qs_z(A, z + 2, x, y, qez[4], qvx[4], qvy[4]);
-    const long long i = cell(g, z, x, y);
-    const bool zs = slab_s(z, nz, np);
-
-    // ---- x- and y-axis Q values at the neighbours
-    float xex[4], xvz[4], xvy[4];  // x-1 .. x+2 (ex) and x-2 .. x+1 (vz, vy)
-    {
-      float e[5], vz5[5], vy5[5];
+  int buf = 0;
+  for (int z = z0; z < z1; ++z, buf ^= 1) {
+    qez[4] = qvx[4] = qvy[4] = 0.f;
+    if (act) qs_z(A, z + 2, x, y, qez[4], qvx[4], qvy[4]);
+    float ox[3] = {0.f, 0.f, 0.f}, oy[3] = {0.f, 0.f, 0.f};
+    GS G{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (act) G = qs_own(A, z, x, y, ox, oy);
 #pragma unroll
-      for (int k = 0; k < 5; ++k) qs_x(A, z, x - 2 + k, y, e[k], vz5[k], vy5[k]);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) { xex[k] = e[k + 1]; xvz[k] = vz5[k]; xvy[k] = vy5[k]; }
+    for (int k = 0; k < 3; ++k) { sqx[buf][k][ty + 2][tx] = ox[k]; sqy[buf][k][ty][tx + 2] = oy[k]; }
+    if (ty < 4) {
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+      if (yin) qs_x(A, z, hxn, y, h0, h1, h2);
+      sqx[buf][0][hr][tx] = h0; sqx[buf][1][hr][tx] = h1; sqx[buf][2][hr][tx] = h2;
     }
-    float yey[4], yvz[4], yvx[4];
-    {
-      float e[5], vz5[5], vx5[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) qs_y(A, z, x, y - 2 + k, e[k], vz5[k], vx5[k]);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) { yey[k] = e[k + 1]; yvz[k] = vz5[k]; yvx[k] = vx5[k]; }
+    if (tx < 4) {
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+      if (xin) qs_y(A, z, x, hyn, h0, h1, h2);
+      sqy[buf][0][ty][hc] = h0; sqy[buf][1][ty][hc] = h1; sqy[buf][2][ty][hc] = h2;
     }
+    __syncthreads();
 
-    // ---- adjoint velocities
-    const float dvz = -dplus(qez[1], qez[2], qez[3], qez[4]) * idz -
-                      dminus(xvz[0], xvz[1], xvz[2], xvz[3]) * idx -
-                      dminus(yvz[0], yvz[1], yvz[2], yvz[3]) * idy;
-    const float dvx = -dplus(xex[0], xex[1], xex[2], xex[3]) * idx -
-                      dminus(qvx[0], qvx[1], qvx[2], qvx[3]) * idz -
-                      dminus(yvx[0], yvx[1], yvx[2], yvx[3]) * idy;
-    const float dvy = -dplus(yey[0], yey[1], yey[2], yey[3]) * idy -
-                      dminus(xvy[0], xvy[1], xvy[2], xvy[3]) * idx -
-                      dminus(qvy[0], qvy[1], qvy[2], qvy[3]) * idz;
+    if (act) {
+      const int i = cell32(g, z, x, y);
+      const float(*QX)[BX + 4][32] = sqx[buf];
+      const float(*QY)[BX][36] = sqy[buf];
+      // ---- adjoint velocities
+      const float dvz = -dplus(qez[1], qez[2], qez[3], qez[4]) * idz -
+                        dminus(QX[1][ty][tx], QX[1][ty + 1][tx], QX[1][ty + 2][tx], QX[1][ty + 3][tx]) * idx -
+                        dminus(QY[1][ty][tx], QY[1][ty][tx + 1], QY[1][ty][tx + 2], QY[1][ty][tx + 3]) * idy;
+      const float dvx = -dplus(QX[0][ty + 1][tx], QX[0][ty + 2][tx], QX[0][ty + 3][tx], QX[0][ty + 4][tx]) * idx -
+                        dminus(qvx[0], qvx[1], qvx[2], qvx[3]) * idz -
+                        dminus(QY[2][ty][tx], QY[2][ty][tx + 1], QY[2][ty][tx + 2], QY[2][ty][tx + 3]) * idy;
+      const float dvy = -dplus(QY[0][ty][tx + 1], QY[0][ty][tx + 2], QY[0][ty][tx + 3], QY[0][ty][tx + 4]) * idy -
+                        dminus(QX[2][ty][tx], QX[2][ty + 1][tx], QX[2][ty + 2][tx], QX[2][ty + 3][tx]) * idx -
+                        dminus(qvy[0], qvy[1], qvy[2], qvy[3]) * idz;
 
-    // ---- images from the forward velocities of the same step
-    const float *vz = A.f.vz, *vx = A.f.vx, *vy = A.f.vy;
-    float ezz = dminus(vz[i - 2 * sz], vz[i - sz], vz[i], vz[i + sz]) * idz;
-    float exx = dminus(vx[i - 2 * sx], vx[i - sx], vx[i], vx[i + sx]) * idx;
-    float eyy = dminus(vy[i - 2], vy[i - 1], vy[i], vy[i + 1]) * idy;
-    float dvx_dz = dplus(vx[i - sz], vx[i], vx[i + sz], vx[i + 2 * sz]) * idz;
-    float dvy_dz = dplus(vy[i - sz], vy[i], vy[i + sz], vy[i + 2 * sz]) * idz;
-    float dvx_dy = dplus(vx[i - 1], vx[i], vx[i + 1], vx[i + 2]) * idy;
-    float dvz_dx = dplus(vz[i - sx], vz[i], vz[i + sx], vz[i + 2 * sx]) * idx;
-    float dvz_dy = dplus(vz[i - 1], vz[i], vz[i + 1], vz[i + 2]) * idy;
-    float dvy_dx = dplus(vy[i - sx], vy[i], vy[i + sx], vy[i + 2 * sx]) * idx;
-    const GS G = gs_at(A, i);
-    if (zs) {
-      const float *c = g.cz;
-      const float Kz = c[CK * nz + z], az = c[CA * nz + z], bz = c[CB * nz + z];
-      const float Kzh = c[CKH * nz + z], azh = c[CAH * nz + z], bzh = c[CBH * nz + z];
-      const long long k = psi_z_idx(g, z, x, y);
-      const float *p = A.ps.z;
-      ezz = ezz * Kz + (bz * p[PSI_VA * g.slab_z + k] + az * ezz);
-      dvx_dz = dvx_dz * Kzh + (bzh * p[PSI_VB1 * g.slab_z + k] + azh * dvx_dz);
-      dvy_dz = dvy_dz * Kzh + (bzh * p[PSI_VB2 * g.slab_z + k] + azh * dvy_dz);
-      A.lout.z[PSI_VA * g.slab_z + k] = bz * (A.lin.z[PSI_VA * g.slab_z + k] + G.ez);
-      A.lout.z[PSI_VB1 * g.slab_z + k] = bzh * (A.lin.z[PSI_VB1 * g.slab_z + k] + G.xz);
-      A.lout.z[PSI_VB2 * g.slab_z + k] = bzh * (A.lin.z[PSI_VB2 * g.slab_z + k] + G.yz);
+      // ---- images from the forward velocities of the same step
+      const float *vz = A.f.vz, *vx = A.f.vx, *vy = A.f.vy;
+      float ezz = dminus(vz[i - 2 * sz], vz[i - sz], vz[i], vz[i + sz]) * idz;
+      float exx = dminus(vx[i - 2 * sx], vx[i - sx], vx[i], vx[i + sx]) * idx;
+      float eyy = dminus(vy[i - 2], vy[i - 1], vy[i], vy[i + 1]) * idy;
+      float dvx_dz = dplus(vx[i - sz], vx[i], vx[i + sz], vx[i + 2 * sz]) * idz;
+      float dvy_dz = dplus(vy[i - sz], vy[i], vy[i + sz], vy[i + 2 * sz]) * idz;
+      float dvx_dy = dplus(vx[i - 1], vx[i], vx[i + 1], vx[i + 2]) * idy;
+      float dvz_dx = dplus(vz[i - sx], vz[i], vz[i + sx], vz[i + 2 * sx]) * idx;
+      float dvz_dy = dplus(vz[i - 1], vz[i], vz[i + 1], vz[i + 2]) * idy;
+      float dvy_dx = dplus(vy[i - sx], vy[i], vy[i + sx], vy[i + 2 * sx]) * idx;
+      if (slab_s(z, nz, np)) {
+        const float *c = g.cz;
+        const float Kz = c[CK * nz + z], az = c[CA * nz + z], bz = c[CB * nz + z];
+        const float Kzh = c[CKH * nz + z], azh = c[CAH * nz + z], bzh = c[CBH * nz + z];
+        const int k = psi32_z(g, z, x, y);
+        const float *p = A.ps.z;
+        ezz = ezz * Kz + (bz * p[PSI_VA * (int)g.slab_z + k] + az * ezz);
+        dvx_dz = dvx_dz * Kzh + (bzh * p[PSI_VB1 * (int)g.slab_z + k] + azh * dvx_dz);
+        dvy_dz = dvy_dz * Kzh + (bzh * p[PSI_VB2 * (int)g.slab_z + k] + azh * dvy_dz);
+        A.lout.z[PSI_VA * (int)g.slab_z + k] = bz * (A.lin.z[PSI_VA * (int)g.slab_z + k] + G.ez);
+        A.lout.z[PSI_VB1 * (int)g.slab_z + k] = bzh * (A.lin.z[PSI_VB1 * (int)g.slab_z + k] + G.xz);
+        A.lout.z[PSI_VB2 * (int)g.slab_z + k] = bzh * (A.lin.z[PSI_VB2 * (int)g.slab_z + k] + G.yz);
+      }
+      if (xs) {
+        const float *c = g.cx;
+        const float Kx = c[CK * nx + x], ax = c[CA * nx + x], bx = c[CB * nx + x];
+        const float Kxh = c[CKH * nx + x], axh = c[CAH * nx + x], bxh = c[CBH * nx + x];
+        const int k = psi32_x(g, z, x, y);
+        const float *p = A.ps.x;
+        exx = exx * Kx + (bx * p[PSI_VA * (int)g.slab_x + k] + ax * exx);
+        dvz_dx = dvz_dx * Kxh + (bxh * p[PSI_VB1 * (int)g.slab_x + k] + axh * dvz_dx);
+        dvy_dx = dvy_dx * Kxh + (bxh * p[PSI_VB2 * (int)g.slab_x + k] + axh * dvy_dx);
+        A.lout.x[PSI_VA * (int)g.slab_x + k] = bx * (A.lin.x[PSI_VA * (int)g.slab_x + k] + G.ex);
+        A.lout.x[PSI_VB1 * (int)g.slab_x + k] = bxh * (A.lin.x[PSI_VB1 * (int)g.slab_x + k] + G.xz);
+        A.lout.x[PSI_VB2 * (int)g.slab_x + k] = bxh * (A.lin.x[PSI_VB2 * (int)g.slab_x + k] + G.xy);
+      }
+      if (ys) {
+        const float *c = g.cy;
+        const float Ky = c[CK * ny + y], ay = c[CA * ny + y], by = c[CB * ny + y];
+        const float Kyh = c[CKH * ny + y], ayh = c[CAH * ny + y], byh = c[CBH * ny + y];
+        const int k = psi32_y(g, z, x, y);
+        const float *p = A.ps.y;
+        eyy = eyy * Ky + (by * p[PSI_VA * (int)g.slab_y + k] + ay * eyy);
+        dvz_dy = dvz_dy * Kyh + (byh * p[PSI_VB1 * (int)g.slab_y + k] + ayh * dvz_dy);
+        dvx_dy = dvx_dy * Kyh + (byh * p[PSI_VB2 * (int)g.slab_y + k] + ayh * dvx_dy);
+        A.lout.y[PSI_VA * (int)g.slab_y + k] = by * (A.lin.y[PSI_VA * (int)g.slab_y + k] + G.ey);
+        A.lout.y[PSI_VB1 * (int)g.slab_y + k] = byh * (A.lin.y[PSI_VB1 * (int)g.slab_y + k] + G.yz);
+        A.lout.y[PSI_VB2 * (int)g.slab_y + k] = byh * (A.lin.y[PSI_VB2 * (int)g.slab_y + k] + G.xy);
+      }
+      if (A.g0) {
+        const float azz = A.a.szz[i], axx = A.a.sxx[i], ayy = A.a.syy[i];
+        const float axz = A.a.sxz[i], axy = A.a.sxy[i], ayz = A.a.syz[i];
+        A.g0[i] += (azz + axx + ayy) * (ezz + exx + eyy) * dt;
+        A.g1[i] += (2.0f * (azz * ezz + axx * exx + ayy * eyy) + axz * (dvx_dz + dvz_dx) +
+                    axy * (dvx_dy + dvy_dx) + ayz * (dvy_dz + dvz_dy)) * dt;
+      }
+      A.a.vz[i] += dvz;
+      A.a.vx[i] += dvx;
+      A.a.vy[i] += dvy;
     }
-    if (xs) {
-      const float *c = g.cx;
-      const float Kx = c[CK * nx + x], ax = c[CA * nx + x], bx = c[CB * nx + x];
-      const float Kxh = c[CKH * nx + x], axh = c[CAH * nx + x], bxh = c[CBH * nx + x];
-      const long long k = psi_x_idx(g, z, x, y);
-      const float *p = A.ps.x;
-      exx = exx * Kx + (bx * p[PSI_VA * g.slab_x + k] + ax * exx);
-      dvz_dx = dvz_dx * Kxh + (bxh * p[PSI_VB1 * g.slab_x + k] + axh * dvz_dx);
-      dvy_dx = dvy_dx * Kxh + (bxh * p[PSI_VB2 * g.slab_x + k] + axh * dvy_dx);
-      A.lout.x[PSI_VA * g.slab_x + k] = bx * (A.lin.x[PSI_VA * g.slab_x + k] + G.ex);
-      A.lout.x[PSI_VB1 * g.slab_x + k] = bxh * (A.lin.x[PSI_VB1 * g.slab_x + k] + G.xz);
-      A.lout.x[PSI_VB2 * g.slab_x + k] = bxh * (A.lin.x[PSI_VB2 * g.slab_x + k] + G.xy);
-    }
-    if (ys) {
-      const float *c = g.cy;
-      const float Ky = c[CK * ny + y], ay = c[CA * ny + y], by = c[CB * ny + y];
-      const float Kyh = c[CKH * ny + y], ayh = c[CAH * ny + y], byh = c[CBH * ny + y];
-      const long long k = psi_y_idx(g, z, x, y);
-      const float *p = A.ps.y;
-      eyy = eyy * Ky + (by * p[PSI_VA * g.slab_y + k] + ay * eyy);
-      dvz_dy = dvz_dy * Kyh + (byh * p[PSI_VB1 * g.slab_y + k] + ayh * dvz_dy);
-      dvx_dy = dvx_dy * Kyh + (byh * p[PSI_VB2 * g.slab_y + k] + ayh * dvx_dy);
-      A.lout.y[PSI_VA * g.slab_y + k] = by * (A.lin.y[PSI_VA * g.slab_y + k] + G.ey);
-      A.lout.y[PSI_VB1 * g.slab_y + k] = byh * (A.lin.y[PSI_VB1 * g.slab_y + k] + G.yz);
-      A.lout.y[PSI_VB2 * g.slab_y + k] = byh * (A.lin.y[PSI_VB2 * g.slab_y + k] + G.xy);
-    }
-    if (A.g0) {
-      const float azz = A.a.szz[i], axx = A.a.sxx[i], ayy = A.a.syy[i];
-      const float axz = A.a.sxz[i], axy = A.a.sxy[i], ayz = A.a.syz[i];
-      A.g0[i] += (azz + axx + ayy) * (ezz + exx + eyy) * dt;
-      A.g1[i] += (2.0f * (azz * ezz + axx * exx + ayy * eyy) + axz * (dvx_dz + dvz_dx) +
-                  axy * (dvx_dy + dvy_dx) + ayz * (dvy_dz + dvz_dy)) * dt;
-    }
-    A.a.vz[i] += dvz;
-    A.a.vx[i] += dvx;
-    A.a.vy[i] += dvy;
-
 #pragma unroll
     for (int k = 0; k < 4; ++k) { qez[k] = qez[k + 1]; qvx[k] = qvx[k + 1]; qvy[k] = qvy[k + 1]; }
   }
@@ -258,7 +314,7 @@ __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int z
 
 // ---------------------------------------------------------- velocity stage
 // G of the velocity stage at cell n: adjoint velocity * buoyancy * dt.
-__device__ __forceinline__ void gv_at(const ExactArgs &A, long long n, float &gz, float &gx,
+__device__ __forceinline__ void gv_at(const ExactArgs &A, int n, float &gz, float &gx,
                                       float &gy) {
   const float s = A.buoy[n] * A.g.dt;
   gz = A.a.vz[n] * s;
@@ -273,14 +329,14 @@ __device__ __forceinline__ void qv_z(const ExactArgs &A, int zn, int x, int y, f
   const Geo &g = A.g;
   if (zn < 2 || zn > g.nz - 3) { qzz = qxz = qyz = 0.f; return; }
   float gz, gx, gy;
-  gv_at(A, cell(g, zn, x, y), gz, gx, gy);
+  gv_at(A, cell32(g, zn, x, y), gz, gx, gy);
   if (slab_s(zn, g.nz, g.np)) {
-    const long long k = psi_z_idx(g, zn, x, y);
+    const int k = psi32_z(g, zn, x, y);
     const float *c = g.cz;
     const int nz = g.nz;
-    qzz = qpml(gz, true, A.lin.z[PSI_SAA * g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
-    qxz = qpml(gx, true, A.lin.z[PSI_SAB1 * g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
-    qyz = qpml(gy, true, A.lin.z[PSI_SAB2 * g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+    qzz = qpml(gz, true, A.lin.z[PSI_SAA * (int)g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+    qxz = qpml(gx, true, A.lin.z[PSI_SAB1 * (int)g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+    qyz = qpml(gy, true, A.lin.z[PSI_SAB2 * (int)g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
   } else {
     qzz = gz; qxz = gx; qyz = gy;
   }
@@ -293,14 +349,14 @@ __device__ __forceinline__ void qv_x(const ExactArgs &A, int z, int xn, int y, f
   const Geo &g = A.g;
   if (xn < 2 || xn > g.nx - 3) { qxz = qxx = qxy = 0.f; return; }
   float gz, gx, gy;
-  gv_at(A, cell(g, z, xn, y), gz, gx, gy);
+  gv_at(A, cell32(g, z, xn, y), gz, gx, gy);
   if (slab_v(xn, g.nx, g.np)) {
-    const long long k = psi_x_idx(g, z, xn, y);
+    const int k = psi32_x(g, z, xn, y);
     const float *c = g.cx;
     const int nx = g.nx;
-    qxz = qpml(gz, true, A.lin.x[PSI_SAB1 * g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
-    qxx = qpml(gx, true, A.lin.x[PSI_SAA * g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
-    qxy = qpml(gy, true, A.lin.x[PSI_SAB2 * g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+    qxz = qpml(gz, true, A.lin.x[PSI_SAB1 * (int)g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+    qxx = qpml(gx, true, A.lin.x[PSI_SAA * (int)g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+    qxy = qpml(gy, true, A.lin.x[PSI_SAB2 * (int)g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
   } else {
     qxz = gz; qxx = gx; qxy = gy;
   }
@@ -313,123 +369,175 @@ __device__ __forceinline__ void qv_y(const ExactArgs &A, int z, int x, int yn, f
   const Geo &g = A.g;
   if (yn < 2 || yn > g.ny - 3) { qyz = qxy = qyy = 0.f; return; }
   float gz, gx, gy;
-  gv_at(A, cell(g, z, x, yn), gz, gx, gy);
+  gv_at(A, cell32(g, z, x, yn), gz, gx, gy);
   if (slab_v(yn, g.ny, g.np)) {
-    const long long k = psi_y_idx(g, z, x, yn);
+    const int k = psi32_y(g, z, x, yn);
     const float *c = g.cy;
     const int ny = g.ny;
-    qyz = qpml(gz, true, A.lin.y[PSI_SAB1 * g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
-    qxy = qpml(gx, true, A.lin.y[PSI_SAB2 * g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
-    qyy = qpml(gy, true, A.lin.y[PSI_SAA * g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+    qyz = qpml(gz, true, A.lin.y[PSI_SAB1 * (int)g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qxy = qpml(gx, true, A.lin.y[PSI_SAB2 * (int)g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qyy = qpml(gy, true, A.lin.y[PSI_SAA * (int)g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
   } else {
     qyz = gz; qxy = gx; qyy = gy;
   }
 }
 
+// Own cell of the velocity stage: G and the Q of its x- and y-axis terms
+// (qx: vz <- sxz, vx <- sxx, vy <- sxy; qy: vz <- syz, vx <- sxy, vy <- syy).
+__device__ __forceinline__ void qv_own(const ExactArgs &A, int z, int x, int y, float &gz,
+                                       float &gx, float &gy, float qx[3], float qy[3]) {
+  const Geo &g = A.g;
+  gv_at(A, cell32(g, z, x, y), gz, gx, gy);
+  if (slab_v(x, g.nx, g.np)) {
+    const int k = psi32_x(g, z, x, y);
+    const float *c = g.cx;
+    const int nx = g.nx;
+    qx[0] = qpml(gz, true, A.lin.x[PSI_SAB1 * (int)g.slab_x + k], c[CK * nx + x], c[CA * nx + x]);
+    qx[1] = qpml(gx, true, A.lin.x[PSI_SAA * (int)g.slab_x + k], c[CKH * nx + x], c[CAH * nx + x]);
+    qx[2] = qpml(gy, true, A.lin.x[PSI_SAB2 * (int)g.slab_x + k], c[CK * nx + x], c[CA * nx + x]);
+  } else {
+    qx[0] = gz; qx[1] = gx; qx[2] = gy;
+  }
+  if (slab_v(y, g.ny, g.np)) {
+    const int k = psi32_y(g, z, x, y);
+    const float *c = g.cy;
+    const int ny = g.ny;
+    qy[0] = qpml(gz, true, A.lin.y[PSI_SAB1 * (int)g.slab_y + k], c[CK * ny + y], c[CA * ny + y]);
+    qy[1] = qpml(gx, true, A.lin.y[PSI_SAB2 * (int)g.slab_y + k], c[CK * ny + y], c[CA * ny + y]);
+    qy[2] = qpml(gy, true, A.lin.y[PSI_SAA * (int)g.slab_y + k], c[CKH * ny + y], c[CAH * ny + y]);
+  } else {
+    qy[0] = gz; qy[1] = gx; qy[2] = gy;
+  }
+}
+
+// Same staging as k_adj_stress_exact.
 template <int BX>
 __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int zchunk, int nzc) {
+  __shared__ float sqx[2][3][BX + 4][32];
+  __shared__ float sqy[2][3][BX][36];
   const Geo &g = A.g;
-  const int y = blockIdx.x * 32 + threadIdx.x;
-  const int x = blockIdx.y * BX + threadIdx.y;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int y = blockIdx.x * 32 + tx;
+  const int x = blockIdx.y * BX + ty;
   const int z0 = max((int)blockIdx.z * zchunk, 2);
   const int z1 = min((int)blockIdx.z * zchunk + zchunk, g.nz - 2);
   (void)nzc;
-  if (x < 2 || x > g.nx - 3 || y < 2 || y > g.ny - 3 || z0 >= z1) return;
+  if (z0 >= z1) return;  // uniform over the CTA
   const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
-  const long long sz = g.sz;
+  const int sz = (int)g.sz;
   const int sx = g.sx;
   const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
+  const bool xin = x >= 2 && x <= nx - 3, yin = y >= 2 && y <= ny - 3;
+  const bool act = xin && yin;
   const bool xs = slab_v(x, nx, np), ys = slab_v(y, ny, np);
+  const int hr = ty < 2 ? ty : BX + ty;
+  const int hxn = (int)blockIdx.y * BX - 2 + hr;
+  const int hc = tx < 2 ? tx : 32 + tx;
+  const int hyn = (int)blockIdx.x * 32 - 2 + hc;
 
-  // z-axis Q values of planes z-2 .. z+2
   float qzz[5], qxz[5], qyz[5];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) qv_z(A, z0 - 2 + k, x, y, qzz[k], qxz[k], qyz[k]);
+  for (int k = 0; k < 4; ++k) {
+    qzz[k] = qxz[k] = qyz[k] = 0.f;
+    if (act) qv_z(A, z0 - 2 + k, x, y, qzz[k], qxz[k], qyz[k]);
+  }
 
-  for (int z = z0; z < z1; ++z) {
-    qv_z(A, z + 2, x, y, qzz[4], qxz[4], qyz[4]);
-    const long long i = cell(g, z, x, y);
-    const bool zs = slab_s(z, nz, np);
-
-    float x_xz[5], x_xx[5], x_xy[5];  // x-2 .. x+2
+  int buf = 0;
+  for (int z = z0; z < z1; ++z, buf ^= 1) {
+    qzz[4] = qxz[4] = qyz[4] = 0.f;
+    if (act) qv_z(A, z + 2, x, y, qzz[4], qxz[4], qyz[4]);
+    float ox[3] = {0.f, 0.f, 0.f}, oy[3] = {0.f, 0.f, 0.f};
+    float gz = 0.f, gx = 0.f, gy = 0.f;
+    if (act) qv_own(A, z, x, y, gz, gx, gy, ox, oy);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) qv_x(A, z, x - 2 + k, y, x_xz[k], x_xx[k], x_xy[k]);
-    float y_yz[5], y_xy[5], y_yy[5];  // y-2 .. y+2
-#pragma unroll
-    for (int k = 0; k < 5; ++k) qv_y(A, z, x, y - 2 + k, y_yz[k], y_xy[k], y_yy[k]);
+    for (int k = 0; k < 3; ++k) { sqx[buf][k][ty + 2][tx] = ox[k]; sqy[buf][k][ty][tx + 2] = oy[k]; }
+    if (ty < 4) {
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+      if (yin) qv_x(A, z, hxn, y, h0, h1, h2);
+      sqx[buf][0][hr][tx] = h0; sqx[buf][1][hr][tx] = h1; sqx[buf][2][hr][tx] = h2;
+    }
+    if (tx < 4) {
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+      if (xin) qv_y(A, z, x, hyn, h0, h1, h2);
+      sqy[buf][0][ty][hc] = h0; sqy[buf][1][ty][hc] = h1; sqy[buf][2][ty][hc] = h2;
+    }
+    __syncthreads();
 
-    // ---- adjoint stresses
-    const float dszz = -dminus(qzz[0], qzz[1], qzz[2], qzz[3]) * idz;
-    const float dsxx = -dminus(x_xx[0], x_xx[1], x_xx[2], x_xx[3]) * idx;
-    const float dsyy = -dminus(y_yy[0], y_yy[1], y_yy[2], y_yy[3]) * idy;
-    const float dsxz = -dplus(x_xz[1], x_xz[2], x_xz[3], x_xz[4]) * idx -
-                       dplus(qxz[1], qxz[2], qxz[3], qxz[4]) * idz;
-    const float dsyz = -dplus(y_yz[1], y_yz[2], y_yz[3], y_yz[4]) * idy -
-                       dplus(qyz[1], qyz[2], qyz[3], qyz[4]) * idz;
-    const float dsxy = -dplus(y_xy[1], y_xy[2], y_xy[3], y_xy[4]) * idy +
-                       dq_t(x_xy[2], x_xy[3], x_xy[4]) * idx;
+    if (act) {
+      const int i = cell32(g, z, x, y);
+      const float(*QX)[BX + 4][32] = sqx[buf];
+      const float(*QY)[BX][36] = sqy[buf];
+      // ---- adjoint stresses (x: 0 vz<-sxz, 1 vx<-sxx, 2 vy<-sxy;
+      //                        y: 0 vz<-syz, 1 vx<-sxy, 2 vy<-syy)
+      const float dszz = -dminus(qzz[0], qzz[1], qzz[2], qzz[3]) * idz;
+      const float dsxx = -dminus(QX[1][ty][tx], QX[1][ty + 1][tx], QX[1][ty + 2][tx], QX[1][ty + 3][tx]) * idx;
+      const float dsyy = -dminus(QY[2][ty][tx], QY[2][ty][tx + 1], QY[2][ty][tx + 2], QY[2][ty][tx + 3]) * idy;
+      const float dsxz = -dplus(QX[0][ty + 1][tx], QX[0][ty + 2][tx], QX[0][ty + 3][tx], QX[0][ty + 4][tx]) * idx -
+                         dplus(qxz[1], qxz[2], qxz[3], qxz[4]) * idz;
+      const float dsyz = -dplus(QY[0][ty][tx + 1], QY[0][ty][tx + 2], QY[0][ty][tx + 3], QY[0][ty][tx + 4]) * idy -
+                         dplus(qyz[1], qyz[2], qyz[3], qyz[4]) * idz;
+      const float dsxy = -dplus(QY[1][ty][tx + 1], QY[1][ty][tx + 2], QY[1][ty][tx + 3], QY[1][ty][tx + 4]) * idy +
+                         dq_t(QX[2][ty + 2][tx], QX[2][ty + 3][tx], QX[2][ty + 4][tx]) * idx;
 
-    // ---- buoyancy image from the forward stresses of the same step
-    const float *szz = A.f.szz, *sxx = A.f.sxx, *syy = A.f.syy;
-    const float *sxz = A.f.sxz, *sxy = A.f.sxy, *syz = A.f.syz;
-    float dszz_dz = dplus(szz[i - sz], szz[i], szz[i + sz], szz[i + 2 * sz]) * idz;
-    float dsxz_dx = dminus(sxz[i - 2 * sx], sxz[i - sx], sxz[i], sxz[i + sx]) * idx;
-    float dsyz_dy = dminus(syz[i - 2], syz[i - 1], syz[i], syz[i + 1]) * idy;
-    float dsxz_dz = dminus(sxz[i - 2 * sz], sxz[i - sz], sxz[i], sxz[i + sz]) * idz;
-    float dsxx_dx = dplus(sxx[i - sx], sxx[i], sxx[i + sx], sxx[i + 2 * sx]) * idx;
-    float dsxy_dy = dminus(sxy[i - 2], sxy[i - 1], sxy[i], sxy[i + 1]) * idy;
-    float dsyz_dz = dminus(syz[i - 2 * sz], syz[i - sz], syz[i], syz[i + sz]) * idz;
-    float dsxy_dx = (EFWI_C1 * (sxy[i] - sxy[i - sx]) - EFWI_C2 * (sxy[i - sx] - sxy[i - 2 * sx])) * idx;
-    float dsyy_dy = dplus(syy[i - 1], syy[i], syy[i + 1], syy[i + 2]) * idy;
-    float gz, gx, gy;
-    gv_at(A, i, gz, gx, gy);
-    if (zs) {
-      const float *c = g.cz;
-      const float Kz = c[CK * nz + z], bz = c[CB * nz + z], Kzh = c[CKH * nz + z], bzh = c[CBH * nz + z];
-      const long long k = psi_z_idx(g, z, x, y);
-      const float *p = A.ps.z;
-      dszz_dz = dszz_dz * Kzh + p[PSI_SAA * g.slab_z + k];
-      dsxz_dz = dsxz_dz * Kz + p[PSI_SAB1 * g.slab_z + k];
-      dsyz_dz = dsyz_dz * Kz + p[PSI_SAB2 * g.slab_z + k];
-      A.lout.z[PSI_SAA * g.slab_z + k] = bzh * (A.lin.z[PSI_SAA * g.slab_z + k] + gz);
-      A.lout.z[PSI_SAB1 * g.slab_z + k] = bz * (A.lin.z[PSI_SAB1 * g.slab_z + k] + gx);
-      A.lout.z[PSI_SAB2 * g.slab_z + k] = bz * (A.lin.z[PSI_SAB2 * g.slab_z + k] + gy);
+      // ---- buoyancy image from the forward stresses of the same step
+      const float *szz = A.f.szz, *sxx = A.f.sxx, *syy = A.f.syy;
+      const float *sxz = A.f.sxz, *sxy = A.f.sxy, *syz = A.f.syz;
+      float dszz_dz = dplus(szz[i - sz], szz[i], szz[i + sz], szz[i + 2 * sz]) * idz;
+      float dsxz_dx = dminus(sxz[i - 2 * sx], sxz[i - sx], sxz[i], sxz[i + sx]) * idx;
+      float dsyz_dy = dminus(syz[i - 2], syz[i - 1], syz[i], syz[i + 1]) * idy;
+      float dsxz_dz = dminus(sxz[i - 2 * sz], sxz[i - sz], sxz[i], sxz[i + sz]) * idz;
+      float dsxx_dx = dplus(sxx[i - sx], sxx[i], sxx[i + sx], sxx[i + 2 * sx]) * idx;
+      float dsxy_dy = dminus(sxy[i - 2], sxy[i - 1], sxy[i], sxy[i + 1]) * idy;
+      float dsyz_dz = dminus(syz[i - 2 * sz], syz[i - sz], syz[i], syz[i + sz]) * idz;
+      float dsxy_dx = (EFWI_C1 * (sxy[i] - sxy[i - sx]) - EFWI_C2 * (sxy[i - sx] - sxy[i - 2 * sx])) * idx;
+      float dsyy_dy = dplus(syy[i - 1], syy[i], syy[i + 1], syy[i + 2]) * idy;
+      if (slab_s(z, nz, np)) {
+        const float *c = g.cz;
+        const float Kz = c[CK * nz + z], bz = c[CB * nz + z], Kzh = c[CKH * nz + z], bzh = c[CBH * nz + z];
+        const int k = psi32_z(g, z, x, y);
+        const float *p = A.ps.z;
+        dszz_dz = dszz_dz * Kzh + p[PSI_SAA * (int)g.slab_z + k];
+        dsxz_dz = dsxz_dz * Kz + p[PSI_SAB1 * (int)g.slab_z + k];
+        dsyz_dz = dsyz_dz * Kz + p[PSI_SAB2 * (int)g.slab_z + k];
+        A.lout.z[PSI_SAA * (int)g.slab_z + k] = bzh * (A.lin.z[PSI_SAA * (int)g.slab_z + k] + gz);
+        A.lout.z[PSI_SAB1 * (int)g.slab_z + k] = bz * (A.lin.z[PSI_SAB1 * (int)g.slab_z + k] + gx);
+        A.lout.z[PSI_SAB2 * (int)g.slab_z + k] = bz * (A.lin.z[PSI_SAB2 * (int)g.slab_z + k] + gy);
+      }
+      if (xs) {
+        const float *c = g.cx;
+        const float Kx = c[CK * nx + x], bx = c[CB * nx + x], Kxh = c[CKH * nx + x], bxh = c[CBH * nx + x];
+        const int k = psi32_x(g, z, x, y);
+        const float *p = A.ps.x;
+        dsxz_dx = dsxz_dx * Kx + p[PSI_SAB1 * (int)g.slab_x + k];
+        dsxx_dx = dsxx_dx * Kxh + p[PSI_SAA * (int)g.slab_x + k];
+        dsxy_dx = dsxy_dx * Kx + p[PSI_SAB2 * (int)g.slab_x + k];
+        A.lout.x[PSI_SAB1 * (int)g.slab_x + k] = bx * (A.lin.x[PSI_SAB1 * (int)g.slab_x + k] + gz);
+        A.lout.x[PSI_SAA * (int)g.slab_x + k] = bxh * (A.lin.x[PSI_SAA * (int)g.slab_x + k] + gx);
+        A.lout.x[PSI_SAB2 * (int)g.slab_x + k] = bx * (A.lin.x[PSI_SAB2 * (int)g.slab_x + k] + gy);
+      }
+      if (ys) {
+        const float *c = g.cy;
+        const float Ky = c[CK * ny + y], by = c[CB * ny + y], Kyh = c[CKH * ny + y], byh = c[CBH * ny + y];
+        const int k = psi32_y(g, z, x, y);
+        const float *p = A.ps.y;
+        dsyz_dy = dsyz_dy * Ky + p[PSI_SAB1 * (int)g.slab_y + k];
+        dsxy_dy = dsxy_dy * Ky + p[PSI_SAB2 * (int)g.slab_y + k];
+        dsyy_dy = dsyy_dy * Kyh + p[PSI_SAA * (int)g.slab_y + k];
+        A.lout.y[PSI_SAB1 * (int)g.slab_y + k] = by * (A.lin.y[PSI_SAB1 * (int)g.slab_y + k] + gz);
+        A.lout.y[PSI_SAB2 * (int)g.slab_y + k] = by * (A.lin.y[PSI_SAB2 * (int)g.slab_y + k] + gx);
+        A.lout.y[PSI_SAA * (int)g.slab_y + k] = byh * (A.lin.y[PSI_SAA * (int)g.slab_y + k] + gy);
+      }
+      if (A.g0) {
+        A.g0[i] += (A.a.vz[i] * (dszz_dz + dsxz_dx + dsyz_dy) + A.a.vx[i] * (dsxz_dz + dsxx_dx + dsxy_dy) +
+                    A.a.vy[i] * (dsyz_dz + dsxy_dx + dsyy_dy)) * dt;
+      }
+      A.a.szz[i] += dszz;
+      A.a.sxx[i] += dsxx;
+      A.a.syy[i] += dsyy;
+      A.a.sxz[i] += dsxz;
+      A.a.syz[i] += dsyz;
+      A.a.sxy[i] += dsxy;
     }
-    if (xs) {
-      const float *c = g.cx;
-      const float Kx = c[CK * nx + x], bx = c[CB * nx + x], Kxh = c[CKH * nx + x], bxh = c[CBH * nx + x];
-      const long long k = psi_x_idx(g, z, x, y);
-      const float *p = A.ps.x;
-      dsxz_dx = dsxz_dx * Kx + p[PSI_SAB1 * g.slab_x + k];
-      dsxx_dx = dsxx_dx * Kxh + p[PSI_SAA * g.slab_x + k];
-      dsxy_dx = dsxy_dx * Kx + p[PSI_SAB2 * g.slab_x + k];
-      A.lout.x[PSI_SAB1 * g.slab_x + k] = bx * (A.lin.x[PSI_SAB1 * g.slab_x + k] + gz);
-      A.lout.x[PSI_SAA * g.slab_x + k] = bxh * (A.lin.x[PSI_SAA * g.slab_x + k] + gx);
-      A.lout.x[PSI_SAB2 * g.slab_x + k] = bx * (A.lin.x[PSI_SAB2 * g.slab_x + k] + gy);
-    }
-    if (ys) {
-      const float *c = g.cy;
-      const float Ky = c[CK * ny + y], by = c[CB * ny + y], Kyh = c[CKH * ny + y], byh = c[CBH * ny + y];
-      const long long k = psi_y_idx(g, z, x, y);
-      const float *p = A.ps.y;
-      dsyz_dy = dsyz_dy * Ky + p[PSI_SAB1 * g.slab_y + k];
-      dsxy_dy = dsxy_dy * Ky + p[PSI_SAB2 * g.slab_y + k];
-      dsyy_dy = dsyy_dy * Kyh + p[PSI_SAA * g.slab_y + k];
-      A.lout.y[PSI_SAB1 * g.slab_y + k] = by * (A.lin.y[PSI_SAB1 * g.slab_y + k] + gz);
-      A.lout.y[PSI_SAB2 * g.slab_y + k] = by * (A.lin.y[PSI_SAB2 * g.slab_y + k] + gx);
-      A.lout.y[PSI_SAA * g.slab_y + k] = byh * (A.lin.y[PSI_SAA * g.slab_y + k] + gy);
-    }
-    if (A.g0) {
-      A.g0[i] += (A.a.vz[i] * (dszz_dz + dsxz_dx + dsyz_dy) + A.a.vx[i] * (dsxz_dz + dsxx_dx + dsxy_dy) +
-                  A.a.vy[i] * (dsyz_dz + dsxy_dx + dsyy_dy)) * dt;
-    }
-    A.a.szz[i] += dszz;
-    A.a.sxx[i] += dsxx;
-    A.a.syy[i] += dsyy;
-    A.a.sxz[i] += dsxz;
-    A.a.syz[i] += dsyz;
-    A.a.sxy[i] += dsxy;
-
 #pragma unroll
     for (int k = 0; k < 4; ++k) { qzz[k] = qzz[k + 1]; qxz[k] = qxz[k + 1]; qyz[k] = qyz[k + 1]; }
   }
@@ -437,12 +545,20 @@ __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int
 
 }  // namespace
 
-void launch_adj_stress_exact(dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk, int nzc) {
-  k_adj_stress_exact<4><<<grid, dim3(32, 4), 0, st>>>(A, zchunk, nzc);
+void launch_adj_stress_exact(int bx, dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk,
+                             int nzc) {
+  if (bx == 8)
+    k_adj_stress_exact<8><<<grid, dim3(32, 8), 0, st>>>(A, zchunk, nzc);
+  else
+    k_adj_stress_exact<4><<<grid, dim3(32, 4), 0, st>>>(A, zchunk, nzc);
 }
 
-void launch_adj_velocity_exact(dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk, int nzc) {
-  k_adj_velocity_exact<4><<<grid, dim3(32, 4), 0, st>>>(A, zchunk, nzc);
+void launch_adj_velocity_exact(int bx, dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk,
+                               int nzc) {
+  if (bx == 8)
+    k_adj_velocity_exact<8><<<grid, dim3(32, 8), 0, st>>>(A, zchunk, nzc);
+  else
+    k_adj_velocity_exact<4><<<grid, dim3(32, 4), 0, st>>>(A, zchunk, nzc);
 }
 
 // rho image from the buoyancy image: B = 1/rho on [2, n-3]^3

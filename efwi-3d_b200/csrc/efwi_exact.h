@@ -16,9 +16,11 @@ struct ExactArgs {
 
 // Transpose of the stress stage of step k (+ lambda/mu images), then of the
 // velocity stage of step k-1 (+ buoyancy image); the grid is
-// (ceil(ny/32), ceil(nx/4), ceil(nz/zchunk)) with 32 x 4 threads.
-void launch_adj_stress_exact(dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk, int nzc);
-void launch_adj_velocity_exact(dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk, int nzc);
+// (ceil(ny/32), ceil(nx/bx), ceil(nz/zchunk)) with 32 x bx threads, bx 4 or 8.
+void launch_adj_stress_exact(int bx, dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk,
+                             int nzc);
+void launch_adj_velocity_exact(int bx, dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk,
+                               int nzc);
 
 __global__ void k_buoy_to_rho(const float *gB, const float *buoy, float *grho, int nz, int nx,
                               int ny, int py);
