@@ -21,7 +21,7 @@ ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, "libefwi.so")
 BUILD = os.path.join(PKG, "_build")
 SOURCES = ["efwi_fwd.cu", "efwi_fwd_tma.cu", "efwi_rev.cu", "efwi_rev_tma.cu", "efwi_aux.cu",
-           "efwi_abi.cu", "efwi_noalloc.cu", "efwi_exact.cu"]
+           "efwi_abi.cu", "efwi_noalloc.cu", "efwi_exact.cu", "efwi_cnn.cu"]
 HEADERS = ["efwi_common.cuh", "efwi_kernels.h", "efwi_tma.cuh", "efwi_window.cuh", "efwi_exact.h",
            "efwi_revolve.h"]
 

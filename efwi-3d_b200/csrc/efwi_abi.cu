@@ -606,9 +606,12 @@ ExactArgs exact_args(EfwiHandle *h, const Fields &f, const Psi &ps, const Fields
 //   transpose of stress stage k (+ lambda, mu images)      if k <= nt-2
 //   adjoint source -2 * res at sample k                    if k >= 1
 //   transpose of velocity stage k-1 (+ buoyancy image)     if k >= 1.
-// glam, gmu, gB: pitched image accumulators.
+// glam, gmu, gB: pitched image accumulators.  With `adj_source` set, obs
+// holds the adjoint source itself (the derivative of some objective with
+// respect to the traces, traces layout): no misfit is formed and the source
+// is injected as it is, so the images are J^T applied to it.
 int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res_out,
-               float *glam, float *gmu, float *gB, cudaStream_t st) {
+               float *glam, float *gmu, float *gB, cudaStream_t st, bool adj_source = false) {
   const int nt = h->grid.nt;
   const int ntl = nt_eff(h);
   const long long N = h->N;
@@ -674,6 +677,14 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
       }
     } else {  // CK_BLOCK
       const int k = act.a;
+      if (first && adj_source) {
+        first = false;
+        if (sh.nrec > 0) {
+          k_traces_to_tm<<<dim3((nt + 31) / 32, (sh.nrec + 31) / 32, 3), dim3(32, 8), 0, st>>>(
+              obs, h->res_tm.as<float>(), nt, sh.nrec);
+          h->launches[K_OTHER]++;
+        }
+      }
       if (first) {
         first = false;
         rc = misfit_shot(h, sh, obs, h->traces_tm.as<float>(), h->res_tm.as<float>(), jdev, st);
@@ -693,7 +704,7 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
         if (b.rec.ncell > 0) {
           Timer t(h, K_INJECT, st, k);
           k_inject<<<(b.rec.ncell + 127) / 128, 128, 0, st>>>(a, N, b.rec, h->res_tm.as<float>(), k,
-                                                              -2.0f);
+                                                              adj_source ? 1.0f : -2.0f);
         }
         Timer t(h, K_ADJ_VELOCITY, st, k);
         launch_adj_velocity_exact(bxe, grid, st, exact_args(h, b.f, b.ps, a, par_v, gB, nullptr), zc, nzc);
@@ -929,7 +940,7 @@ int efwi_forward(EfwiHandle *h, int n, const int *ids, float *traces, void *stre
 
 static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs, int mode,
                          double *misfit, float *glam, float *gmu, float *grho, float *res_out,
-                         cudaStream_t st) {
+                         cudaStream_t st, bool adj_source = false) {
   const int nt = h->grid.nt;
   const long long N = h->N;
   const bool grad = glam != nullptr;
@@ -958,7 +969,7 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     for (int k = 0; k < n; ++k) {
       const ShotHost &sh = h->shots[ids[k]];
       int rc = exact_shot(h, ids[k], obs + obs_off, jdev + k, res_out ? res_out + obs_off : nullptr,
-                          glam, gmu, grho, st);
+                          glam, gmu, grho, st, adj_source);
       if (rc) return rc;
       obs_off += 3LL * sh.nrec * nt;
     }
@@ -1106,6 +1117,61 @@ int efwi_gradient(EfwiHandle *h, int n, const int *ids, const float *obs, int mo
   if (mode != EFWI_MODE_REFERENCE && mode != EFWI_MODE_EXACT)
     return fail(h, EFWI_ERR_ARG, "gradient mode %d is not available", mode);
   return gradient_impl(h, n, ids, obs, mode, misfit, glam, gmu, grho, res, (cudaStream_t)stream);
+}
+
+int efwi_adjoint(EfwiHandle *h, int n, const int *ids, const float *adj_src, float *g_lam,
+                 float *g_mu, float *g_rho, void *stream) {
+  int rc = check_ready(h, n, ids);
+  if (rc) return rc;
+  if (n > 0 && !adj_src) return fail(h, EFWI_ERR_ARG, "null adjoint source");
+  if (!g_lam || !g_mu || !g_rho) return fail(h, EFWI_ERR_ARG, "null gradient output");
+  return gradient_impl(h, n, ids, adj_src, EFWI_MODE_EXACT, nullptr, g_lam, g_mu, g_rho, nullptr,
+                       (cudaStream_t)stream, true);
+}
+
+int efwi_illumination(EfwiHandle *h, int n, const int *ids, float *h_lam, float *h_mu,
+                      float *h_rho, void *stream) {
+  int rc = check_ready(h, n, ids);
+  if (rc) return rc;
+  if (!h_lam || !h_mu || !h_rho) return fail(h, EFWI_ERR_ARG, "null illumination output");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long N = h->N;
+  const int nt = h->grid.nt;
+  rc = status_reset(h, st);
+  if (rc) return rc;
+  CK_CUDA(h, h->grad.ensure(sizeof(float) * 3 * N));
+  CK_CUDA(h, cudaMemsetAsync(h->grad.p, 0, sizeof(float) * 3 * N, st));
+  float *il = h->grad.as<float>(), *im = il + N, *ib = il + 2 * N;
+  for (int b0 = 0; b0 < n; b0 += h->max_batch) {
+    const int S = std::min(h->max_batch, n - b0);
+    long long ntr = 0;
+    for (int s = 0; s < S; ++s) ntr += 3LL * h->shots[ids[b0 + s]].nrec * nt;
+    CK_CUDA(h, h->traces_tm.ensure(sizeof(float) * std::max(ntr, 1LL)));
+    Batch b;
+    rc = prepare_batch(h, ids + b0, S, h->traces_tm.as<float>(), ntr, st, &b);
+    if (rc) return rc;
+    RecArgs norec = b.rec;
+    norec.ncell = 0;
+    const int ntl = nt_eff(h);
+    const dim3 grid((h->grid.ny + 31) / 32, (h->grid.nx + 3) / 4, (h->grid.nz - 4 + 7) / 8);
+    for (int it = 0; it <= ntl - 2; ++it) {
+      b.src.it = it;
+      rc = forward_step(h, b.f, b.ps, S, b.src, norec, nullptr, st, it, b.mp);
+      if (rc) return rc;
+      Timer t(h, K_OTHER, st, it);
+      k_illumination<<<grid, dim3(32, 4), 0, st>>>(h->geo, b.f, b.ps, S, h->buoy.as<float>(),
+                                                   it + 1 <= ntl - 2, il, im, ib);
+    }
+  }
+  const EfwiGrid &G = h->grid;
+  k_buoy_to_rho_sq<<<1184, 256, 0, st>>>(ib, h->buoy.as<float>(), G.nz, G.nx, G.ny, h->py);
+  k_pitch_copy<<<1184, 256, 0, st>>>(il, h_lam, G.nz, G.nx, G.ny, h->py, 0);
+  k_pitch_copy<<<1184, 256, 0, st>>>(im, h_mu, G.nz, G.nx, G.ny, h->py, 0);
+  k_pitch_copy<<<1184, 256, 0, st>>>(ib, h_rho, G.nz, G.nx, G.ny, h->py, 0);
+  h->launches[K_OTHER] += 4;
+  rc = check_launch(h, "illumination");
+  if (rc) return rc;
+  return status_check(h, st);
 }
 
 int efwi_set_checkpoint_budget(EfwiHandle *h, long long bytes) {

@@ -577,6 +577,133 @@ __global__ void k_buoy_to_rho(const float *gB, const float *buoy, float *grho, i
   }
 }
 
+// Source illumination (diagonal pseudo-Hessian of Shin et al. 2001): for the
+// state S_k after forward step k-1, adds at every cell of [2, n-3]^3, summed
+// over the S shots of the batch,
+//   hl += 3 (dt div)^2                       (d sigma_ii / d lambda = dt div)
+//   hm += dt^2 (4 sum_i e_ii^2 + sum_i<j (e_ij + e_ji)^2)
+//   hb += dt^2 |modified stress divergence|^2 (d v / d B)
+// from the C-PML-modified derivatives of the forward step: the stress-stage
+// terms of step k (velocities and stress memory variables of S_k, when
+// do_stress) and the velocity-stage terms of step k-1 (stresses and updated
+// velocity memory variables of S_k).  Grid (ceil(ny/32), ceil(nx/4),
+// ceil((nz-4)/8)), 32 x 4 threads; each thread sums its shots in order.
+__global__ void __launch_bounds__(128)
+k_illumination(Geo g, Fields f, Psi ps, int S, const float *buoy, int do_stress, float *hl,
+               float *hm, float *hb) {
+  const int y = blockIdx.x * 32 + threadIdx.x;
+  const int x = blockIdx.y * 4 + threadIdx.y;
+  const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
+  if (x < 2 || x > nx - 3 || y < 2 || y > ny - 3) return;
+  const int z0 = 2 + (int)blockIdx.z * 8, z1 = min(z0 + 8, nz - 2);
+  const int sz = (int)g.sz, sx = g.sx;
+  const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy, dt2 = dt * dt;
+  const bool xs = slab_s(x, nx, np), ys = slab_s(y, ny, np);
+  const bool xv = slab_v(x, nx, np), yv = slab_v(y, ny, np);
+  for (int z = z0; z < z1; ++z) {
+    const int i = cell32(g, z, x, y);
+    const bool zs = slab_s(z, nz, np);
+    float al = 0.f, am = 0.f, ab = 0.f;
+    for (int s = 0; s < S; ++s) {
+      const long long so = (long long)s * g.N;
+      const float *pz = ps.z + (long long)s * 6 * g.slab_z;
+      const float *px = ps.x + (long long)s * 6 * g.slab_x;
+      const float *py = ps.y + (long long)s * 6 * g.slab_y;
+      if (do_stress) {
+        const float *vz = f.vz + so, *vx = f.vx + so, *vy = f.vy + so;
+        float ezz = dminus(vz[i - 2 * sz], vz[i - sz], vz[i], vz[i + sz]) * idz;
+        float exx = dminus(vx[i - 2 * sx], vx[i - sx], vx[i], vx[i + sx]) * idx;
+        float eyy = dminus(vy[i - 2], vy[i - 1], vy[i], vy[i + 1]) * idy;
+        float dvx_dz = dplus(vx[i - sz], vx[i], vx[i + sz], vx[i + 2 * sz]) * idz;
+        float dvy_dz = dplus(vy[i - sz], vy[i], vy[i + sz], vy[i + 2 * sz]) * idz;
+        float dvx_dy = dplus(vx[i - 1], vx[i], vx[i + 1], vx[i + 2]) * idy;
+        float dvz_dx = dplus(vz[i - sx], vz[i], vz[i + sx], vz[i + 2 * sx]) * idx;
+        float dvz_dy = dplus(vz[i - 1], vz[i], vz[i + 1], vz[i + 2]) * idy;
+        float dvy_dx = dplus(vy[i - sx], vy[i], vy[i + sx], vy[i + 2 * sx]) * idx;
+        if (zs) {
+          const float *c = g.cz;
+          const int k = psi32_z(g, z, x, y), sl = (int)g.slab_z;
+          ezz = ezz * c[CK * nz + z] + (c[CB * nz + z] * pz[PSI_VA * sl + k] + c[CA * nz + z] * ezz);
+          dvx_dz = dvx_dz * c[CKH * nz + z] + (c[CBH * nz + z] * pz[PSI_VB1 * sl + k] + c[CAH * nz + z] * dvx_dz);
+          dvy_dz = dvy_dz * c[CKH * nz + z] + (c[CBH * nz + z] * pz[PSI_VB2 * sl + k] + c[CAH * nz + z] * dvy_dz);
+        }
+        if (xs) {
+          const float *c = g.cx;
+          const int k = psi32_x(g, z, x, y), sl = (int)g.slab_x;
+          exx = exx * c[CK * nx + x] + (c[CB * nx + x] * px[PSI_VA * sl + k] + c[CA * nx + x] * exx);
+          dvz_dx = dvz_dx * c[CKH * nx + x] + (c[CBH * nx + x] * px[PSI_VB1 * sl + k] + c[CAH * nx + x] * dvz_dx);
+          dvy_dx = dvy_dx * c[CKH * nx + x] + (c[CBH * nx + x] * px[PSI_VB2 * sl + k] + c[CAH * nx + x] * dvy_dx);
+        }
+        if (ys) {
+          const float *c = g.cy;
+          const int k = psi32_y(g, z, x, y), sl = (int)g.slab_y;
+          eyy = eyy * c[CK * ny + y] + (c[CB * ny + y] * py[PSI_VA * sl + k] + c[CA * ny + y] * eyy);
+          dvz_dy = dvz_dy * c[CKH * ny + y] + (c[CBH * ny + y] * py[PSI_VB1 * sl + k] + c[CAH * ny + y] * dvz_dy);
+          dvx_dy = dvx_dy * c[CKH * ny + y] + (c[CBH * ny + y] * py[PSI_VB2 * sl + k] + c[CAH * ny + y] * dvx_dy);
+        }
+        const float div = ezz + exx + eyy;
+        const float exz = dvx_dz + dvz_dx, exy = dvx_dy + dvy_dx, eyz = dvy_dz + dvz_dy;
+        al += 3.0f * div * div * dt2;
+        am += (4.0f * (ezz * ezz + exx * exx + eyy * eyy) + exz * exz + exy * exy + eyz * eyz) * dt2;
+      }
+      const float *szz = f.szz + so, *sxx = f.sxx + so, *syy = f.syy + so;
+      const float *sxz = f.sxz + so, *sxy = f.sxy + so, *syz = f.syz + so;
+      float dszz_dz = dplus(szz[i - sz], szz[i], szz[i + sz], szz[i + 2 * sz]) * idz;
+      float dsxz_dx = dminus(sxz[i - 2 * sx], sxz[i - sx], sxz[i], sxz[i + sx]) * idx;
+      float dsyz_dy = dminus(syz[i - 2], syz[i - 1], syz[i], syz[i + 1]) * idy;
+      float dsxz_dz = dminus(sxz[i - 2 * sz], sxz[i - sz], sxz[i], sxz[i + sz]) * idz;
+      float dsxx_dx = dplus(sxx[i - sx], sxx[i], sxx[i + sx], sxx[i + 2 * sx]) * idx;
+      float dsxy_dy = dminus(sxy[i - 2], sxy[i - 1], sxy[i], sxy[i + 1]) * idy;
+      float dsyz_dz = dminus(syz[i - 2 * sz], syz[i - sz], syz[i], syz[i + sz]) * idz;
+      float dsxy_dx = (EFWI_C1 * (sxy[i] - sxy[i - sx]) - EFWI_C2 * (sxy[i - sx] - sxy[i - 2 * sx])) * idx;
+      float dsyy_dy = dplus(syy[i - 1], syy[i], syy[i + 1], syy[i + 2]) * idy;
+      if (zs) {
+        const float *c = g.cz;
+        const int k = psi32_z(g, z, x, y), sl = (int)g.slab_z;
+        dszz_dz = dszz_dz * c[CKH * nz + z] + pz[PSI_SAA * sl + k];
+        dsxz_dz = dsxz_dz * c[CK * nz + z] + pz[PSI_SAB1 * sl + k];
+        dsyz_dz = dsyz_dz * c[CK * nz + z] + pz[PSI_SAB2 * sl + k];
+      }
+      if (xv) {
+        const float *c = g.cx;
+        const int k = psi32_x(g, z, x, y), sl = (int)g.slab_x;
+        dsxz_dx = dsxz_dx * c[CK * nx + x] + px[PSI_SAB1 * sl + k];
+        dsxx_dx = dsxx_dx * c[CKH * nx + x] + px[PSI_SAA * sl + k];
+        dsxy_dx = dsxy_dx * c[CK * nx + x] + px[PSI_SAB2 * sl + k];
+      }
+      if (yv) {
+        const float *c = g.cy;
+        const int k = psi32_y(g, z, x, y), sl = (int)g.slab_y;
+        dsyz_dy = dsyz_dy * c[CK * ny + y] + py[PSI_SAB1 * sl + k];
+        dsxy_dy = dsxy_dy * c[CK * ny + y] + py[PSI_SAB2 * sl + k];
+        dsyy_dy = dsyy_dy * c[CKH * ny + y] + py[PSI_SAA * sl + k];
+      }
+      const float qz = dszz_dz + dsxz_dx + dsyz_dy, qx = dsxz_dz + dsxx_dx + dsxy_dy,
+                  qy = dsyz_dz + dsxy_dx + dsyy_dy;
+      ab += (qz * qz + qx * qx + qy * qy) * dt2;
+    }
+    hl[i] += al;
+    hm[i] += am;
+    hb[i] += ab;
+  }
+  (void)buoy;
+}
+
+// Illumination of rho from that of the buoyancy: (dB/drho)^2 = B^4 on
+// [2, n-3]^3 (Model.cu:65-76), 0 elsewhere; in place.
+__global__ void k_buoy_to_rho_sq(float *hb, const float *buoy, int nz, int nx, int ny, int py) {
+  const long long n = (long long)nz * nx * py;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % py);
+    const long long zx = i / py;
+    const int x = (int)(zx % nx), z = (int)(zx / nx);
+    const bool in = z >= 2 && z <= nz - 3 && x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3;
+    const float b2 = buoy[i] * buoy[i];
+    hb[i] = in ? hb[i] * b2 * b2 : 0.0f;
+  }
+}
+
 // State of the oracle's layout, [27][nz][nx][ny] (9 fields, then the 18
 // memory variables in the order m_vz_z m_vz_x m_vz_y m_vx_z m_vx_x m_vx_y
 // m_vy_z m_vy_x m_vy_y m_szz_z m_sxx_x m_syy_y m_sxz_z m_sxz_x m_sxy_x

@@ -75,6 +75,10 @@ _SIGS = {
     "efwi_misfit_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    "efwi_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_void_p]),
+    "efwi_illumination": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_set_checkpoint_budget": (C.c_int, [C.c_void_p, C.c_longlong]),
     "efwi_state_bytes": (C.c_longlong, [C.c_void_p]),
     "efwi_checkpoint_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
@@ -82,6 +86,10 @@ _SIGS = {
                                        C.POINTER(C.c_int), C.POINTER(C.c_int),
                                        C.POINTER(C.c_int), C.c_int]),
     "efwi_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "efwi_conv3d_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                      C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "efwi_conv3d_wgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                    C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "efwi_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "efwi_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong),
                                     C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

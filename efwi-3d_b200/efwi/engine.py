@@ -232,6 +232,35 @@ class Propagator:
             return J.value, gl, gm, gr, res
         return J.value, gl, gm, gr
 
+    def adjoint(self, shot_ids, adj_src: torch.Tensor):
+        """J^T adj_src: exact adjoint images (lambda, mu, rho) of the shots
+        for an adjoint source in the traces layout."""
+        ids = self._ids(shot_ids)
+        w = _f32_dev(adj_src, self.device)
+        if w.numel() != sum(self.trace_sizes(ids)):
+            raise ValueError("adjoint source size does not match the shots")
+        shp = self.grid.shape
+        gl, gm, gr = (torch.empty(shp, device=self.device, dtype=torch.float32) for _ in range(3))
+        with torch.cuda.device(self.device):
+            rc = self._L.efwi_adjoint(self._h, len(ids), ids.ctypes.data_as(C.POINTER(C.c_int)),
+                                      C.c_void_p(w.data_ptr()), C.c_void_p(gl.data_ptr()),
+                                      C.c_void_p(gm.data_ptr()), C.c_void_p(gr.data_ptr()),
+                                      self._stream())
+        check(self._h, rc)
+        return gl, gm, gr
+
+    def illumination(self, shot_ids):
+        """Diagonal pseudo-Hessian (source illumination) of lambda, mu, rho."""
+        ids = self._ids(shot_ids)
+        shp = self.grid.shape
+        hl, hm, hr = (torch.empty(shp, device=self.device, dtype=torch.float32) for _ in range(3))
+        with torch.cuda.device(self.device):
+            rc = self._L.efwi_illumination(self._h, len(ids), ids.ctypes.data_as(C.POINTER(C.c_int)),
+                                           C.c_void_p(hl.data_ptr()), C.c_void_p(hm.data_ptr()),
+                                           C.c_void_p(hr.data_ptr()), self._stream())
+        check(self._h, rc)
+        return hl, hm, hr
+
     # ------------------------------------------------- exact-adjoint support
     def set_checkpoint_budget(self, nbytes: int) -> None:
         """HBM bytes for the exact gradient's checkpoint slots."""

@@ -120,6 +120,23 @@ int efwi_gradient(EfwiHandle *h, int n, const int *shot_ids, const float *obs, i
                   double *misfit, float *g_lam, float *g_mu, float *g_rho, float *res,
                   void *stream);
 
+/* J^T applied to an adjoint source (no reference counterpart): the exact
+ * adjoint of the forward modelling of the shots, with the device traces
+ * adj_src (traces layout, the derivative of some objective with respect to
+ * the synthetic traces) injected at the receivers, checkpointed as in
+ * EFWI_MODE_EXACT.  g_lam, g_mu, g_rho as in efwi_gradient.  Serves
+ * random-probe estimates of diag(J^T J) (E[(J^T w)^2] for white w). */
+int efwi_adjoint(EfwiHandle *h, int n, const int *shot_ids, const float *adj_src, float *g_lam,
+                 float *g_mu, float *g_rho, void *stream);
+
+/* Source illumination: the diagonal pseudo-Hessian of Shin et al. (2001),
+ * summed over the shots and time steps -- at every cell the squared
+ * derivative of the forward step with respect to lambda, mu and rho
+ * applied to the forward wavefield.  No reference counterpart.  Outputs:
+ * device [nz][nx][ny], overwritten. */
+int efwi_illumination(EfwiHandle *h, int n, const int *shot_ids, float *h_lam, float *h_mu,
+                      float *h_rho, void *stream);
+
 /* Exact-gradient checkpoints (no reference counterpart; the reference keeps
  * only the boundary shell, Boundary.cu).  bytes: HBM for checkpoint slots
  * (default 4 GiB); one slot holds one state of efwi_state_bytes(h) bytes.
@@ -165,6 +182,22 @@ int efwi_misfit_noalloc(int nrec, int nt, float dt, int if_win, const float *win
                         const float *win_end, const float *weights, float src_weight,
                         const float *obs, const float *syn, float *res, double *misfit,
                         void *stream);
+
+/* Learned gradient preconditioner: 3x3x3 convolutions with 16 input and 16
+ * output channels on BF16 tensor cores, FP32 accumulation (no reference
+ * counterpart).  x, y_bf16: device [D][H][W][16] bf16 (channels last);
+ * w: device [27][16 co][16 ci] bf16, tap (dz+1)*9 + (dy+1)*3 + (dx+1);
+ * bias: device [16] f32 or NULL.  Zero padding of 1, stride 1.
+ * efwi_conv3d_forward: y = relu?(conv(x, w) + bias) into y_bf16 and/or
+ * y_f32 ([D][H][W][16] f32); with w'[t][a][b] = w[26-t][b][a] it gives the
+ * gradient of the input.  efwi_conv3d_wgrad: dw[t][co][ci] = sum over
+ * voxels of dy[v][co] x[v + off_t][ci] (f32), through `nparts` partial sums
+ * of 27*256 floats each in `partial`, added in a fixed order.  Return 0, 1
+ * (bad argument) or 2 (launch error). */
+int efwi_conv3d_forward(const void *x, const void *w, const float *bias, int D, int H, int W,
+                        int relu, void *y_bf16, float *y_f32, void *stream);
+int efwi_conv3d_wgrad(const void *x, const void *dy, int D, int H, int W, float *partial,
+                      int nparts, float *dw, void *stream);
 
 /* Per-kernel timing with CUDA events on the call's stream (every
  * `sample`-th time step; 0 disables).  efwi_profile_read fills, for each

@@ -290,6 +290,69 @@ struct Solver {
         }
   }
 
+  // Source illumination of the current state S_k (after forward step k-1):
+  // squared model derivatives of the stress stage of step k (when
+  // do_stress) and of the velocity stage of step k-1 (Shin et al. 2001
+  // pseudo-Hessian); same modified derivatives as stress_fwd/velocity_fwd,
+  // with the stress memory variables advanced as the stress stage would.
+  void illum(double *hl, double *hm, double *hb, bool do_stress) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int z = 2; z <= nz - 3; ++z)
+      for (int x = 2; x <= nx - 3; ++x)
+        for (int y = 2; y <= ny - 3; ++y) {
+          size_t i = idx(z, x, y);
+          const double dt2 = dt * dt;
+          if (do_stress) {
+            double ezz = Dm(vz.data(), i, sz) / dz, exx = Dm(vx.data(), i, sx) / dx, eyy = Dm(vy.data(), i, 1) / dy;
+            double dvx_dz = Dp(vx.data(), i, sz) / dz, dvx_dy = Dp(vx.data(), i, 1) / dy;
+            double dvz_dx = Dp(vz.data(), i, sx) / dx, dvz_dy = Dp(vz.data(), i, 1) / dy;
+            double dvy_dx = Dp(vy.data(), i, sx) / dx, dvy_dz = Dp(vy.data(), i, sz) / dz;
+            if (slabS(z, nz)) {
+              ezz = ezz / pz.K[z] + (pz.b[z] * m_vz_z[i] + pz.a[z] * ezz);
+              dvx_dz = dvx_dz / pz.Kh[z] + (pz.bh[z] * m_vx_z[i] + pz.ah[z] * dvx_dz);
+              dvy_dz = dvy_dz / pz.Kh[z] + (pz.bh[z] * m_vy_z[i] + pz.ah[z] * dvy_dz);
+            }
+            if (slabS(x, nx)) {
+              exx = exx / px.K[x] + (px.b[x] * m_vx_x[i] + px.a[x] * exx);
+              dvz_dx = dvz_dx / px.Kh[x] + (px.bh[x] * m_vz_x[i] + px.ah[x] * dvz_dx);
+              dvy_dx = dvy_dx / px.Kh[x] + (px.bh[x] * m_vy_x[i] + px.ah[x] * dvy_dx);
+            }
+            if (slabS(y, ny)) {
+              eyy = eyy / py.K[y] + (py.b[y] * m_vy_y[i] + py.a[y] * eyy);
+              dvz_dy = dvz_dy / py.Kh[y] + (py.bh[y] * m_vz_y[i] + py.ah[y] * dvz_dy);
+              dvx_dy = dvx_dy / py.Kh[y] + (py.bh[y] * m_vx_y[i] + py.ah[y] * dvx_dy);
+            }
+            double div = ezz + exx + eyy;
+            double exz = dvx_dz + dvz_dx, exy = dvx_dy + dvy_dx, eyz = dvy_dz + dvz_dy;
+            hl[i] += 3.0 * div * div * dt2;
+            hm[i] += (4.0 * (ezz * ezz + exx * exx + eyy * eyy) + exz * exz + exy * exy + eyz * eyz) * dt2;
+          }
+          double q[3];
+          {
+            double a = Dp(szz.data(), i, sz) / dz, b = Dm(sxz.data(), i, sx) / dx, c = Dm(syz.data(), i, 1) / dy;
+            if (slabS(z, nz)) a = a / pz.Kh[z] + m_szz_z[i];
+            if (slabV(x, nx)) b = b / px.K[x] + m_sxz_x[i];
+            if (slabV(y, ny)) c = c / py.K[y] + m_syz_y[i];
+            q[0] = a + b + c;
+          }
+          {
+            double a = Dm(sxz.data(), i, sz) / dz, b = Dp(sxx.data(), i, sx) / dx, c = Dm(sxy.data(), i, 1) / dy;
+            if (slabS(z, nz)) a = a / pz.K[z] + m_sxz_z[i];
+            if (slabV(x, nx)) b = b / px.Kh[x] + m_sxx_x[i];
+            if (slabV(y, ny)) c = c / py.K[y] + m_sxy_y[i];
+            q[1] = a + b + c;
+          }
+          {
+            double a = Dm(syz.data(), i, sz) / dz, b = Dq(sxy.data(), i, sx) / dx, c = Dp(syy.data(), i, 1) / dy;
+            if (slabS(z, nz)) a = a / pz.K[z] + m_syz_z[i];
+            if (slabV(x, nx)) b = b / px.K[x] + m_sxy_x[i];
+            if (slabV(y, ny)) c = c / py.Kh[y] + m_syy_y[i];
+            q[2] = a + b + c;
+          }
+          hb[i] += (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * dt2;
+        }
+  }
+
   // ------------------------------------------------ reference-mode reverse
   // Reverse velocity step on [npml, n-1-npml]^3 with rho imaging
   // (velocity.cu:102-131).
@@ -758,6 +821,43 @@ int oracle_forward(const OracleGrid *g, const double *lam, const double *mu, con
     run_forward(s, shots[k], stf + (size_t)k * g->nt, traces + off, nullptr, nullptr);
     off += (size_t)3 * shots[k].nrec * g->nt;
   }
+  return 0;
+}
+
+// Source illumination (diagonal pseudo-Hessian, Shin et al. 2001) summed
+// over the shots: for every state S_k, k = 1 .. nt-1, the squared
+// derivatives of the forward step with respect to lambda, mu and rho
+// (Solver::illum; rho through B = 1/rho on [2, n-3]^3, (dB/drho)^2 = 1/rho^4).
+int oracle_illumination(const OracleGrid *g, const double *lam, const double *mu,
+                        const double *rho, int nshot, const OracleShot *shots, const double *stf,
+                        double *hl, double *hm, double *hr) {
+  Solver s(*g, lam, mu, rho);
+  const size_t N = s.N;
+  std::fill(hl, hl + N, 0.0);
+  std::fill(hm, hm + N, 0.0);
+  std::vector<double> hb(N, 0.0);
+  const int nt = g->nt;
+  for (int k = 0; k < nshot; ++k) {
+    const OracleShot &sh = shots[k];
+    s.zero_all();
+    std::vector<double> st;
+    taper_stf(stf + (size_t)k * nt, nt, s.dt, st);
+    size_t isrc = s.idx(sh.z_src, sh.x_src, sh.y_src);
+    for (int it = 0; it <= nt - 2; ++it) {
+      s.stress_fwd();
+      double amp = 1500.0 * 1500.0 * st[it] * s.dt;
+      s.szz[isrc] += amp; s.sxx[isrc] += amp; s.syy[isrc] += amp;
+      s.velocity_fwd();
+      s.illum(hl, hm, hb.data(), it + 1 <= nt - 2);
+    }
+  }
+  for (int z = 0; z < s.nz; ++z)
+    for (int x = 0; x < s.nx; ++x)
+      for (int y = 0; y < s.ny; ++y) {
+        size_t i = s.idx(z, x, y);
+        bool in = z >= 2 && z <= s.nz - 3 && x >= 2 && x <= s.nx - 3 && y >= 2 && y <= s.ny - 3;
+        hr[i] = in ? hb[i] / (rho[i] * rho[i] * rho[i] * rho[i]) : 0.0;
+      }
   return 0;
 }
 

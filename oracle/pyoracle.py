@@ -187,6 +187,17 @@ class _Port(_Lib):
         self.lib.oracle_taper_stf(self._p(s), len(s), C.c_double(dt), self._p(out))
         return out
 
+    def illumination(self, case: Case):
+        """Diagonal pseudo-Hessian (source illumination) of lambda, mu, rho."""
+        g, shots = self._grid(case), self._shots(case)
+        lam, mu, rho = self._model(case)
+        stf = np.ascontiguousarray(case.stf, np.float64)
+        out = [np.zeros(lam.shape, np.float64) for _ in range(3)]
+        rc = self.lib.oracle_illumination(C.byref(g), self._p(lam), self._p(mu), self._p(rho),
+                                          case.nshot, shots, self._p(stf), *[self._p(o) for o in out])
+        assert rc == 0
+        return tuple(out)
+
     def step(self, case: Case, state: np.ndarray, amp: float = 0.0, src=(0, 0, 0)) -> np.ndarray:
         g = self._grid(case)
         lam, mu, rho = self._model(case)
