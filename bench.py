@@ -59,6 +59,12 @@ def parse():
                          "steps, tuning --tuning, forward of the true model then one gradient")
     ap.add_argument("--tuning", default="1,4,1,4",
                     help="forward cfg, forward zchunk, reverse cfg, reverse zchunk")
+    ap.add_argument("--iters", type=int, default=20, help="inversion case: L-BFGS iterations")
+    ap.add_argument("--pairs", type=int, default=200, help="inversion case: training pairs")
+    ap.add_argument("--pair-n", type=int, default=40, help="inversion case: model cells of a pair")
+    ap.add_argument("--pair-nt", type=int, default=500)
+    ap.add_argument("--nprobe", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=20)
     return ap.parse_args()
 
 
@@ -272,8 +278,140 @@ def run_case(a):
     print(f"case {a.case}: grid {p.grid.nz}^3, nt {a.nt}, misfit {J:.6e}")
 
 
+def run_inversion(a):
+    """Config 5: learned-step L-BFGS against plain L-BFGS on the config-2
+    problem (vp only), after training the preconditioner on pseudo-Hessian
+    pairs; one JSON line with both misfit-vs-time curves."""
+    import math
+    import torch
+    from efwi import synthetic
+    from efwi.cnn import Preconditioner
+    from efwi.preconditioner import VpObjective, layered_problem, lbfgs, make_pairs, train
+
+    def log(m):
+        print(m, file=sys.stderr, flush=True)
+
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    pairs = make_pairs(a.pairs, n=a.pair_n, nt=a.pair_nt, nprobe=a.nprobe, mode=a.mode, log=log)
+    t_pairs = time.perf_counter() - t0
+    net = Preconditioner(cin=3, seed=0).cuda()
+    t0 = time.perf_counter()
+    hist = train(net, pairs, epochs=a.epochs, log=log)
+    t_train = time.perf_counter() - t0
+    if a.n == 128:
+        prob = synthetic.config2(nt=a.nt, nshot=a.shots, n=a.n)
+    else:
+        prob = layered_problem(n=a.n, nt=a.nt, shots_side=int(round(math.sqrt(a.shots))), seed=7)
+    obj = VpObjective(prob, mode=a.mode)
+    vp0 = torch.from_numpy(prob.vp_init).cuda()
+    plain = lbfgs(obj, vp0, iters=a.iters, log=log)
+    learned = lbfgs(obj, vp0, iters=a.iters, net=net, stop_misfit=plain.misfit[-1], log=log)
+    target = plain.misfit[-1]
+    t_learned = next((t for t, j in zip(learned.seconds, learned.misfit) if j <= target), None)
+    line = {"case": "inversion", "problem": prob.name, "mode": a.mode,
+            "plain": {"misfit": plain.misfit, "seconds": plain.seconds,
+                      "model_rel_l2": plain.model_rel_l2, "evals": plain.evals},
+            "learned": {"misfit": learned.misfit, "seconds": learned.seconds,
+                        "model_rel_l2": learned.model_rel_l2, "evals": learned.evals,
+                        "learned_steps_accepted": learned.learned_accepted},
+            "plain_final_misfit": target, "plain_seconds": plain.seconds[-1],
+            "learned_seconds_to_plain_misfit": t_learned,
+            "time_ratio": (t_learned / plain.seconds[-1]) if t_learned else None,
+            "training": {"pairs": a.pairs, "pair_grid": a.pair_n, "pair_nt": a.pair_nt,
+                         "nprobe": a.nprobe, "epochs": a.epochs, "loss": hist,
+                         "seconds_pairs": t_pairs, "seconds_train": t_train}}
+    print(json.dumps(line))
+
+
+def config4(nt, seed=4, nshot=64):
+    """Config 4: 256 x 256 x 160 model (x, y, z), dx 12.5 m, 64 shots each on
+    an aperture window of lateral extent U[96, 192] cells (seeded), 6 Hz
+    Ricker; layered model with anomalies; C-PML 12 on the global grid and
+    inside every window."""
+    import numpy as np
+    from efwi import synthetic
+    from efwi.engine import Grid, Shot
+    rng = np.random.default_rng(seed)
+    npml, nzm, nxm = 12, 160, 256
+    dt, f0, dx = 1e-3, 6.0, 12.5
+    z = np.arange(nzm)
+    vp1 = np.interp(z, [0, nzm - 1], [1800.0, 4000.0])
+    vp = np.broadcast_to(vp1[:, None, None], (nzm, nxm, nxm)).astype(np.float32).copy()
+    vs = (vp / 1.732).astype(np.float32)
+    rho = (310.0 * vp ** 0.25).astype(np.float32)
+    grid = Grid(nzm + 2 * npml, nxm + 2 * npml, nxm + 2 * npml, npml, nt, dx, dx, dx, dt, f0)
+    shots, wins = [], []
+    for k in range(nshot):
+        L = int(rng.integers(96, 193))
+        cx, cy = (int(v) for v in rng.integers(L // 2, nxm - L // 2, size=2))
+        x0, y0 = cx - L // 2, cy - L // 2
+        xs = np.arange(x0 + 2, x0 + L - 2, 4)
+        X, Y = np.meshgrid(xs, np.arange(y0 + 2, y0 + L - 2, 4), indexing="ij")
+        zr = np.full(X.size, npml + 2, np.int32)
+        shots.append(Shot(src=(npml + 4, cx + npml, cy + npml), z_rec=zr,
+                          x_rec=(X.ravel() + npml).astype(np.int32),
+                          y_rec=(Y.ravel() + npml).astype(np.int32)))
+        wins.append((x0, y0, L + 2 * npml, L + 2 * npml))
+    stf = np.tile(synthetic.ricker(f0, nt, dt), (nshot, 1))
+    return grid, shots, stf, (vp, vs, rho), wins
+
+
+def run_windows(a):
+    """Config 4: 64 shots on uneven windows in one persistent multi-domain
+    launch per half-step, the time loop captured in a CUDA graph; launch
+    shape (tile_bx, zchunk) chosen by the autotuner; one JSON line."""
+    import torch
+    from efwi import synthetic
+    from efwi.autotune import autotune_windows
+    from efwi.engine import Propagator
+    grid, shots, stf, (vp, vs, rho), wins = config4(a.nt)
+    P = Propagator(grid)
+    P.set_survey(shots, stf)
+    lam, mu, rh = synthetic.elastic_params(vp, vs, rho, grid.npml)
+    P.set_model(torch.from_numpy(lam), torch.from_numpy(mu), torch.from_numpy(rh))
+    ids = list(range(len(shots)))
+    tune = autotune_windows(P, ids, wins)
+    for _ in range(max(a.warmup, 1)):
+        P.forward_windows(ids, wins, use_graph=True)
+    torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        P.forward_windows(ids, wins, use_graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / a.steps
+    cells = [grid.nz * w[2] * w[3] for w in wins]
+    steps = grid.nt - 1
+    S = [2 * grid.npml * (w[2] * w[3] + grid.nz * w[3] + grid.nz * w[2]) for w in wins]
+    bytes_step = sum(120 * n + 48 * sl for n, sl in zip(cells, S)) * steps
+    peak, kind = peaks()
+    agg = sum(cells) * steps / (ms * 1e-3) / 1e9
+    print(json.dumps({
+        "case": "windows", "config": {"workload": "config4: 256x256x160 model, dx 12.5 m, 64 shots on "
+                                                  "windows of U[96,192] cells, 6 Hz, forward modelling",
+                                      "nt": grid.nt, "windows": wins, "autotune": tune},
+        "aggregate_gcell_per_s": agg, "per_shot_gcell_per_s_mean": agg / len(wins),
+        "per_shot_cells": cells, "ms_per_call": ms,
+        "roofline": {"bound": "hbm", "achieved": bytes_step / (ms * 1e-3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": bytes_step / (ms * 1e-3) / 1e9 / peak,
+                     "peak_kind": kind, "bytes": "120 N + 48 S per window and step"},
+        "graph": True, "clocks": clocks}))
+    P.close()
+
+
 def main():
     a = parse()
+    if a.case == "inversion":
+        run_inversion(a)
+        return
+    if a.case == "windows":
+        run_windows(a)
+        return
     if a.case:
         run_case(a)
         return

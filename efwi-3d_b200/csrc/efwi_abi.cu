@@ -109,6 +109,9 @@ struct EfwiHandle {
 
   // exact gradient: checkpoint slots and the two adjoint memory-variable sets
   DevBuf ckpt, apsi;
+  // shot windows: per-domain volumes and tables; stream for graph capture
+  DevBuf wvol, wtab;
+  cudaStream_t cap_stream = nullptr;
   long long ck_budget = 4LL << 30;  // bytes of checkpoint slots
   long long ck_forward_steps = 0;   // forward steps of the last exact gradient
   int ck_slots = 0;                 // slots it used
@@ -788,6 +791,7 @@ int efwi_create(const EfwiGrid *g, EfwiHandle **out) {
 void efwi_destroy(EfwiHandle *h) {
   if (!h) return;
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
   delete h;
 }
 
@@ -1117,6 +1121,171 @@ int efwi_gradient(EfwiHandle *h, int n, const int *ids, const float *obs, int mo
   if (mode != EFWI_MODE_REFERENCE && mode != EFWI_MODE_EXACT)
     return fail(h, EFWI_ERR_ARG, "gradient mode %d is not available", mode);
   return gradient_impl(h, n, ids, obs, mode, misfit, glam, gmu, grho, res, (cudaStream_t)stream);
+}
+
+int efwi_forward_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow *win,
+                         float *traces, int use_graph, void *stream) {
+  int rc = check_ready(h, n, ids);
+  if (rc) return rc;
+  if (n > 0 && (!win || !traces)) return fail(h, EFWI_ERR_ARG, "null windows or traces");
+  if (n == 0) return EFWI_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const EfwiGrid &G = h->grid;
+  const int np = G.npml, nz = G.nz, nt = G.nt, bx = h->bx, zchunk = h->zchunk;
+  auto al = [](long long v) { return (v + 63) & ~63LL; };  // 256-byte aligned float offsets
+  std::vector<Domain> dom(n);
+  std::vector<float> coefs;
+  std::vector<long long> vol_off(n), cx_off(n), cy_off(n);
+  std::vector<int> rec_dom, rec_cell, rec_r;
+  long long vol = 0, tr = 0;
+  int tiles = 0;
+  for (int k = 0; k < n; ++k) {
+    const EfwiWindow &w = win[k];
+    const ShotHost &sh = h->shots[ids[k]];
+    if (w.nx < 2 * np + 5 || w.ny < 2 * np + 5 || w.x0 < 0 || w.y0 < 0 || w.x0 + w.nx > G.nx ||
+        w.y0 + w.ny > G.ny)
+      return fail(h, EFWI_ERR_ARG, "window %d (%d+%d, %d+%d) invalid for grid %d x %d, npml %d", k,
+                  w.x0, w.nx, w.y0, w.ny, G.nx, G.ny, np);
+    const long long sc = sh.src_cell;
+    const int sy = (int)(sc % h->py), sx = (int)((sc / h->py) % G.nx), sz = (int)(sc / h->py / G.nx);
+    const int lx = sx - w.x0, ly = sy - w.y0;
+    if (lx < 2 || lx > w.nx - 3 || ly < 2 || ly > w.ny - 3)
+      return fail(h, EFWI_ERR_ARG, "shot %d: source outside the updated part of its window", ids[k]);
+    Domain &d = dom[k];
+    const int pyw = (w.ny + 3) & ~3;
+    Geo &g = d.g;
+    g = h->geo;
+    g.nx = w.nx; g.ny = w.ny;
+    g.N = (long long)nz * w.nx * pyw;
+    g.sz = (long long)w.nx * pyw;
+    g.sx = pyw;
+    g.slab_z = 2LL * np * w.nx * w.ny;
+    g.slab_x = (long long)nz * 2 * np * w.ny;
+    g.slab_y = (long long)nz * w.nx * 2 * np;
+    for (int ax = 0; ax < 2; ++ax) {
+      const int m = ax == 0 ? w.nx : w.ny;
+      std::vector<float> c(6 * m);
+      cpml_profile(m, np, ax == 0 ? G.dx : G.dy, G.f0, G.dt, c.data());
+      for (int i = 0; i < m; ++i) { c[CK * m + i] = 1.0f / c[CK * m + i]; c[CKH * m + i] = 1.0f / c[CKH * m + i]; }
+      (ax == 0 ? cx_off : cy_off)[k] = (long long)coefs.size();
+      coefs.insert(coefs.end(), c.begin(), c.end());
+      while (coefs.size() % 64) coefs.push_back(0.f);
+    }
+    vol_off[k] = vol;
+    vol += al(12 * g.N) + al(psi_per_shot(g));
+    d.src_cell = ((long long)sz * w.nx + lx) * pyw + ly;
+    d.stf = h->stf.as<float>() + (size_t)ids[k] * nt;
+    d.nt = nt;
+    d.tiles_y = (w.ny + 31) / 32;
+    d.tiles_x = (w.nx + bx - 1) / bx;
+    d.nzc = (nz + zchunk - 1) / zchunk;
+    d.tile0 = tiles;
+    tiles += d.tiles_y * d.tiles_x * d.nzc;
+    d.trace_off = tr;
+    d.nrec = sh.nrec;
+    tr += 3LL * sh.nrec * nt;
+    for (int r = 0; r < sh.nrec; ++r) {
+      const long long c = sh.rec_cell[r];
+      const int y = (int)(c % h->py), x = (int)((c / h->py) % G.nx), z = (int)(c / h->py / G.nx);
+      const int xl = x - w.x0, yl = y - w.y0;
+      if (xl < 0 || xl >= w.nx || yl < 0 || yl >= w.ny) continue;
+      rec_dom.push_back(k);
+      rec_cell.push_back((int)(((long long)z * w.nx + xl) * pyw + yl));
+      rec_r.push_back(r);
+    }
+  }
+  CK_CUDA(h, h->wvol.ensure(sizeof(float) * std::max(vol, 1LL)));
+  CK_CUDA(h, h->traces_tm.ensure(sizeof(float) * std::max(tr, 1LL)));
+  const long long nr = (long long)rec_dom.size();
+  const size_t b_dom = ((sizeof(Domain) * n + 255) / 256) * 256, b_coef = sizeof(float) * coefs.size();
+  const size_t b_rec = ((sizeof(int) * nr + 255) / 256) * 256;
+  CK_CUDA(h, h->wtab.ensure(b_dom + b_coef + 3 * b_rec + 256));
+  char *tab = h->wtab.as<char>();
+  float *dcoef = (float *)(tab + b_dom);
+  int *drd = (int *)(tab + b_dom + b_coef), *drc = (int *)((char *)drd + b_rec),
+      *drr = (int *)((char *)drc + b_rec);
+  float *V = h->wvol.as<float>();
+  CK_CUDA(h, cudaMemsetAsync(h->traces_tm.p, 0, sizeof(float) * std::max(tr, 1LL), st));
+  for (int k = 0; k < n; ++k) {
+    Domain &d = dom[k];
+    float *base = V + vol_off[k];
+    d.f = fields_at(base, d.g.N, 1);
+    float *model = base + 9 * d.g.N;
+    d.lam = model; d.mu = model + d.g.N; d.buoy = model + 2 * d.g.N;
+    d.ps = psi_at(base + al(12 * d.g.N), d.g, 1);
+    d.g.cx = dcoef + cx_off[k];
+    d.g.cy = dcoef + cy_off[k];
+    CK_CUDA(h, cudaMemsetAsync(base, 0, sizeof(float) * 9 * d.g.N, st));
+    CK_CUDA(h, cudaMemsetAsync(base + al(12 * d.g.N), 0, sizeof(float) * psi_per_shot(d.g), st));
+    const float *src[3] = {h->lam.as<float>(), h->mu.as<float>(), h->buoy.as<float>()};
+    for (int v = 0; v < 3; ++v)
+      k_window_slice<<<592, 256, 0, st>>>(src[v], model + v * d.g.N, nz, G.nx, h->py, win[k].x0,
+                                          win[k].y0, win[k].nx, win[k].ny, d.g.sx);
+    h->launches[K_OTHER] += 3;
+  }
+  CK_CUDA(h, cudaMemcpyAsync(tab, dom.data(), sizeof(Domain) * n, cudaMemcpyHostToDevice, st));
+  CK_CUDA(h, cudaMemcpyAsync(dcoef, coefs.data(), b_coef, cudaMemcpyHostToDevice, st));
+  if (nr > 0) {
+    CK_CUDA(h, cudaMemcpyAsync(drd, rec_dom.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, st));
+    CK_CUDA(h, cudaMemcpyAsync(drc, rec_cell.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, st));
+    CK_CUDA(h, cudaMemcpyAsync(drr, rec_r.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, st));
+  }
+  rc = check_launch(h, "window set-up");
+  if (rc) return rc;
+  const Domain *ddom = (const Domain *)tab;
+  const int blocks = multi_blocks(bx);
+  const int ntl = nt_eff(h);
+  float *ttm = h->traces_tm.as<float>();
+  auto loop = [&](cudaStream_t s) {
+    for (int it = 0; it <= ntl - 2; ++it) {
+      launch_fwd_multi(bx, blocks, s, ddom, n, tiles, zchunk, it);
+      if (nr > 0) k_record_multi<<<(int)((nr + 127) / 128), 128, 0, s>>>(ddom, drd, drc, drr, (int)nr, ttm, it + 1);
+    }
+  };
+  const long long per_step = 2 + (nr > 0 ? 1 : 0);
+  if (use_graph) {
+    if (!h->cap_stream) CK_CUDA(h, cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+    cudaStream_t cs = h->cap_stream;
+    cudaEvent_t e0, e1;
+    CK_CUDA(h, cudaEventCreateWithFlags(&e0, cudaEventDisableTiming));
+    CK_CUDA(h, cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+    CK_CUDA(h, cudaEventRecord(e0, st));
+    CK_CUDA(h, cudaStreamWaitEvent(cs, e0, 0));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CK_CUDA(h, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    loop(cs);
+    cudaError_t ec = cudaStreamEndCapture(cs, &graph);
+    if (ec == cudaSuccess) ec = cudaGraphInstantiate(&exec, graph, 0);
+    if (ec == cudaSuccess) ec = cudaGraphLaunch(exec, cs);
+    if (ec == cudaSuccess) ec = cudaEventRecord(e1, cs);
+    if (ec == cudaSuccess) ec = cudaStreamWaitEvent(st, e1, 0);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ec != cudaSuccess) return fail(h, EFWI_ERR_CUDA, "graph of the window time loop: %s", cudaGetErrorString(ec));
+  } else {
+    loop(st);
+  }
+  h->launches[K_STRESS_FWD] += ntl - 1;
+  h->launches[K_VELOCITY_FWD] += ntl - 1;
+  if (nr > 0) h->launches[K_RECORD] += ntl - 1;
+  (void)per_step;
+  long long off = 0;
+  for (int k = 0; k < n; ++k) {
+    const int nrs = dom[k].nrec;
+    if (nrs > 0) {
+      k_traces_to_cr_t<<<dim3((nt + 31) / 32, (nrs + 31) / 32, 3), dim3(32, 8), 0, st>>>(
+          ttm + dom[k].trace_off, traces + off, nt, nrs);
+      h->launches[K_OTHER]++;
+    }
+    off += 3LL * nrs * nt;
+  }
+  rc = check_launch(h, "window forward");
+  if (rc) return rc;
+  CK_CUDA(h, cudaStreamSynchronize(st));
+  return EFWI_OK;
 }
 
 int efwi_adjoint(EfwiHandle *h, int n, const int *ids, const float *adj_src, float *g_lam,

@@ -208,3 +208,21 @@ __global__ void k_traces_to_tm(const float *in, float *tm, int nt, int nrec) {
 }
 
 }  // namespace efwi
+
+namespace efwi {
+
+// Copies the window [x0, x0+nxw) x [y0, y0+nyw) (all z) of a pitched global
+// volume (nx, pyg) into a pitched window volume (nxw, pyw); pad columns 0.
+__global__ void k_window_slice(const float *src, float *dst, int nz, int nx, int pyg, int x0,
+                               int y0, int nxw, int nyw, int pyw) {
+  const long long n = (long long)nz * nxw * pyw;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % pyw);
+    const long long zx = i / pyw;
+    const int x = (int)(zx % nxw), z = (int)(zx / nxw);
+    dst[i] = y < nyw ? src[((long long)z * nx + x0 + x) * pyg + y0 + y] : 0.0f;
+  }
+}
+
+}  // namespace efwi

@@ -16,14 +16,13 @@
 
 namespace efwi {
 
-template <int BX>
-__global__ void __launch_bounds__(32 * BX)
-k_stress_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ lam,
-             const float *__restrict__ mu, int zchunk, int nzc, SrcArgs src) {
-  const int y = blockIdx.x * 32 + threadIdx.x;
-  const int x = blockIdx.y * BX + threadIdx.y;
-  const int shot = blockIdx.z / nzc;
-  const int zc = blockIdx.z - shot * nzc;
+// One thread's column (y, x) of z chunk zc of shot `shot`; the kernels
+// below map their launch onto these columns.
+__device__ __forceinline__ void stress_fwd_column(const Geo &g, const Fields &f, const Psi &ps,
+                                                  const float *__restrict__ lam,
+                                                  const float *__restrict__ mu, int y, int x,
+                                                  int shot, int zc, int zchunk,
+                                                  const SrcArgs &src) {
   const int z0 = max(zc * zchunk, 2);
   const int z1 = min(zc * zchunk + zchunk, g.nz - 2);
   if (x < 2 || x > g.nx - 3 || y < 2 || y > g.ny - 3 || z0 >= z1) return;
@@ -136,13 +135,9 @@ k_stress_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ lam,
   }
 }
 
-template <int BX>
-__global__ void __launch_bounds__(32 * BX)
-k_velocity_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ buoy, int zchunk, int nzc) {
-  const int y = blockIdx.x * 32 + threadIdx.x;
-  const int x = blockIdx.y * BX + threadIdx.y;
-  const int shot = blockIdx.z / nzc;
-  const int zc = blockIdx.z - shot * nzc;
+__device__ __forceinline__ void velocity_fwd_column(const Geo &g, const Fields &f, const Psi &ps,
+                                                    const float *__restrict__ buoy, int y, int x,
+                                                    int shot, int zc, int zchunk) {
   const int z0 = max(zc * zchunk, 2);
   const int z1 = min(zc * zchunk + zchunk, g.nz - 2);
   if (x < 2 || x > g.nx - 3 || y < 2 || y > g.ny - 3 || z0 >= z1) return;
@@ -243,6 +238,110 @@ k_velocity_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ buoy, int zchu
       qb3 = sxz[i + 2 * sz];
       qc3 = syz[i + 2 * sz];
     }
+  }
+}
+
+template <int BX>
+__global__ void __launch_bounds__(32 * BX)
+k_stress_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ lam,
+             const float *__restrict__ mu, int zchunk, int nzc, SrcArgs src) {
+  const int shot = blockIdx.z / nzc;
+  stress_fwd_column(g, f, ps, lam, mu, blockIdx.x * 32 + threadIdx.x, blockIdx.y * BX + threadIdx.y,
+                    shot, blockIdx.z - shot * nzc, zchunk, src);
+}
+
+template <int BX>
+__global__ void __launch_bounds__(32 * BX)
+k_velocity_fwd(Geo g, Fields f, Psi ps, const float *__restrict__ buoy, int zchunk, int nzc) {
+  const int shot = blockIdx.z / nzc;
+  velocity_fwd_column(g, f, ps, buoy, blockIdx.x * 32 + threadIdx.x, blockIdx.y * BX + threadIdx.y,
+                      shot, blockIdx.z - shot * nzc, zchunk);
+}
+
+// Several domains of different sizes (shot windows) in one persistent
+// launch: CTA b takes tiles b, b + gridDim.x, ... of the concatenated tile
+// lists; tile t of domain d is (z chunk, x tile, y tile) in that order.
+__device__ __forceinline__ int find_domain(const Domain *dom, int ndom, int t) {
+  int lo = 0, hi = ndom - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (dom[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int BX>
+__global__ void __launch_bounds__(32 * BX)
+k_stress_fwd_multi(const Domain *__restrict__ dom, int ndom, int ntiles, int zchunk, int it) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Domain &d = dom[find_domain(dom, ndom, t)];
+    const int lt = t - d.tile0;
+    const int by = lt % d.tiles_y, r = lt / d.tiles_y;
+    const int bx = r % d.tiles_x, zc = r / d.tiles_x;
+    SrcArgs src{&d.src_cell, d.stf, d.nt, it};
+    stress_fwd_column(d.g, d.f, d.ps, d.lam, d.mu, by * 32 + threadIdx.x, bx * BX + threadIdx.y, 0,
+                      zc, zchunk, src);
+  }
+}
+
+template <int BX>
+__global__ void __launch_bounds__(32 * BX)
+k_velocity_fwd_multi(const Domain *__restrict__ dom, int ndom, int ntiles, int zchunk) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Domain &d = dom[find_domain(dom, ndom, t)];
+    const int lt = t - d.tile0;
+    const int by = lt % d.tiles_y, r = lt / d.tiles_y;
+    const int bx = r % d.tiles_x, zc = r / d.tiles_x;
+    velocity_fwd_column(d.g, d.f, d.ps, d.buoy, by * 32 + threadIdx.x, bx * BX + threadIdx.y, 0, zc,
+                        zchunk);
+  }
+}
+
+// Receivers of all domains (recording, utilities.cu:481-495): receiver u
+// sits at cell rec_cell[u] of domain rec_dom[u] and is receiver rec_r[u] of
+// that domain's shot, whose time-major traces [nt][3][nrec] start at
+// trace_off.  Receivers outside their window are not listed (their traces
+// stay zero).
+__global__ void k_record_multi(const Domain *__restrict__ dom, const int *__restrict__ rec_dom,
+                               const int *__restrict__ rec_cell, const int *__restrict__ rec_r,
+                               int nrec, float *traces_tm, int it) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nrec) return;
+  const Domain &d = dom[rec_dom[u]];
+  const int i = rec_cell[u], r = rec_r[u];
+  float *t = traces_tm + d.trace_off + (long long)it * 3 * d.nrec;
+  t[r] = d.f.vx[i];
+  t[d.nrec + r] = d.f.vy[i];
+  t[2 * d.nrec + r] = d.f.vz[i];
+}
+
+int multi_blocks(int bx) {
+  static int cached[2] = {0, 0};
+  const int k = bx == 8 ? 1 : 0;
+  if (!cached[k]) {
+    int dev = 0, sms = 148, a = 1, b = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (bx == 8) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_stress_fwd_multi<8>, 256, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_velocity_fwd_multi<8>, 256, 0);
+    } else {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_stress_fwd_multi<4>, 128, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_velocity_fwd_multi<4>, 128, 0);
+    }
+    cached[k] = sms * max(1, min(a, b));
+  }
+  return cached[k];
+}
+
+void launch_fwd_multi(int bx, int blocks, cudaStream_t st, const Domain *dom, int ndom, int ntiles,
+                      int zchunk, int it) {
+  if (bx == 8) {
+    k_stress_fwd_multi<8><<<blocks, dim3(32, 8), 0, st>>>(dom, ndom, ntiles, zchunk, it);
+    k_velocity_fwd_multi<8><<<blocks, dim3(32, 8), 0, st>>>(dom, ndom, ntiles, zchunk);
+  } else {
+    k_stress_fwd_multi<4><<<blocks, dim3(32, 4), 0, st>>>(dom, ndom, ntiles, zchunk, it);
+    k_velocity_fwd_multi<4><<<blocks, dim3(32, 4), 0, st>>>(dom, ndom, ntiles, zchunk);
   }
 }
 

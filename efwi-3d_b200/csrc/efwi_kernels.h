@@ -32,6 +32,31 @@ struct RecArgs {
   int ncell;
 };
 
+// One domain of a multi-domain launch (a shot on its own window grid): its
+// geometry, state, model, source and place in the concatenated tile list
+// (tiles_y * tiles_x * nzc tiles from tile0).
+struct Domain {
+  Geo g;
+  Fields f;
+  Psi ps;
+  const float *lam, *mu, *buoy;
+  long long src_cell;
+  const float *stf;  // tapered source-time function [nt]
+  int nt;
+  int tiles_y, tiles_x, nzc, tile0;
+  long long trace_off;  // the shot's time-major traces [nt][3][nrec]
+  int nrec;
+};
+
+// Persistent launches over several domains (L1-served stencils):
+// stress + source, then velocity, for time step `it`; `blocks` CTAs
+// (multi_blocks(bx): the SM count times the resident CTAs per SM).
+int multi_blocks(int bx);
+void launch_fwd_multi(int bx, int blocks, cudaStream_t st, const Domain *dom, int ndom, int ntiles,
+                      int zchunk, int it);
+__global__ void k_record_multi(const Domain *dom, const int *rec_dom, const int *rec_cell,
+                               const int *rec_r, int nrec, float *traces_tm, int it);
+
 // Host launchers of the stencil kernels (bx: x rows per CTA, 4 or 8; the
 // CTA is 32 x bx threads).
 void launch_stress_fwd(int bx, dim3 grid, cudaStream_t st, const Geo &g, const Fields &f,
@@ -77,6 +102,8 @@ void launch_rev_stress_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<23> &
                            const SrcArgs &src, int *status);
 
 __global__ void k_prep_buoyancy(const float *rho, float *buoy, int nz, int nx, int ny, int py);
+__global__ void k_window_slice(const float *src, float *dst, int nz, int nx, int pyg, int x0,
+                               int y0, int nxw, int nyw, int pyw);
 __global__ void k_pitch_copy(const float *src, float *dst, int nz, int nx, int ny, int py,
                              int to_pitched);
 __global__ void k_record(Fields f, long long N, RecArgs rec, float *traces_tm, int it);

@@ -51,6 +51,10 @@ class EfwiShot(C.Structure):
                 ("src_weight", C.c_float)]
 
 
+class EfwiWindow(C.Structure):
+    _fields_ = [("x0", C.c_int), ("y0", C.c_int), ("nx", C.c_int), ("ny", C.c_int)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -75,6 +79,8 @@ _SIGS = {
     "efwi_misfit_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    "efwi_forward_windows": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
+                                       C.c_void_p, C.c_int, C.c_void_p]),
     "efwi_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_illumination": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,

@@ -63,3 +63,27 @@ def autotune(P, shot_id: int, obs_shot: torch.Tensor, nt_probe: int = 16,
             "fwd_ms": round(fwd[bf], 4), "rev_ms": round(rev[br], 4),
             "fwd_default_ms": round(fwd.get((0, 8), float("nan")), 4),
             "rev_default_ms": round(rev.get((0, 8), float("nan")), 4), "probes": len(fwd) + len(rev)}
+
+
+def autotune_windows(P, shot_ids, windows, nt_probe: int = 16, bxs=(4, 8), zchunks=(4, 8, 16)):
+    """Launch shape (tile_bx, zchunk) of the multi-domain window launch: the
+    fastest over short probes (time loop stopped after `nt_probe` steps),
+    timed with CUDA events on the current stream; sets it on P."""
+    P.set_nt_limit(nt_probe)
+    times = {}
+    try:
+        for bx, zc in itertools.product(bxs, zchunks):
+            P.set_options(if_win=P.if_win, tile_bx=bx, zchunk=zc)
+            P.forward_windows(shot_ids, windows, use_graph=True)  # warm
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            P.forward_windows(shot_ids, windows, use_graph=True)
+            e1.record()
+            torch.cuda.synchronize(P.device)
+            times[(bx, zc)] = e0.elapsed_time(e1)
+    finally:
+        P.set_nt_limit(0)
+    best = min(times, key=times.get)
+    P.set_options(if_win=P.if_win, tile_bx=best[0], zchunk=best[1])
+    return {"tile_bx": best[0], "zchunk": best[1], "probe_ms": round(times[best], 3),
+            "probes": len(times)}

@@ -232,6 +232,23 @@ class Propagator:
             return J.value, gl, gm, gr, res
         return J.value, gl, gm, gr
 
+    def forward_windows(self, shot_ids, windows, use_graph: bool = True) -> torch.Tensor:
+        """Traces of shots each on its own window (x0, y0, nx, ny) of the
+        padded grid, all windows in one persistent launch per half-step."""
+        ids = self._ids(shot_ids)
+        if len(windows) != len(ids):
+            raise ValueError("one window per shot")
+        arr = (_lib.EfwiWindow * max(len(ids), 1))()
+        for k, w in enumerate(windows):
+            arr[k].x0, arr[k].y0, arr[k].nx, arr[k].ny = (int(v) for v in w)
+        out = torch.zeros(sum(self.trace_sizes(ids)), device=self.device, dtype=torch.float32)
+        with torch.cuda.device(self.device):
+            rc = self._L.efwi_forward_windows(self._h, len(ids), ids.ctypes.data_as(C.POINTER(C.c_int)),
+                                              C.cast(arr, C.c_void_p), C.c_void_p(out.data_ptr()),
+                                              int(bool(use_graph)), self._stream())
+        check(self._h, rc)
+        return out
+
     def adjoint(self, shot_ids, adj_src: torch.Tensor):
         """J^T adj_src: exact adjoint images (lambda, mu, rho) of the shots
         for an adjoint source in the traces layout."""

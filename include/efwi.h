@@ -120,6 +120,21 @@ int efwi_gradient(EfwiHandle *h, int n, const int *shot_ids, const float *obs, i
                   double *misfit, float *g_lam, float *g_mu, float *g_rho, float *res,
                   void *stream);
 
+/* Shot windows (config 4 of the build's benchmarks; no reference
+ * counterpart): shot k runs on its own aperture window of the padded grid,
+ * x in [x0, x0 + nx), y in [y0, y0 + ny), all z, with its own C-PML of npml
+ * cells inside the window edges; receivers outside the window record
+ * zeros.  All windows of a call advance together in one persistent launch
+ * per half-step (L1-served stencils, tile_bx and zchunk of
+ * efwi_set_options); use_graph = 1 captures the whole time loop in a CUDA
+ * graph and launches it once.  traces: device, concatenation over shot_ids
+ * of [3][nrec][nt].  The call synchronises the stream. */
+typedef struct {
+  int x0, y0, nx, ny;
+} EfwiWindow;
+int efwi_forward_windows(EfwiHandle *h, int n, const int *shot_ids, const EfwiWindow *windows,
+                         float *traces, int use_graph, void *stream);
+
 /* J^T applied to an adjoint source (no reference counterpart): the exact
  * adjoint of the forward modelling of the shots, with the device traces
  * adj_src (traces layout, the derivative of some objective with respect to

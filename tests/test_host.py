@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _header_symbols():
     txt = open(os.path.join(ROOT, "include", "efwi.h")).read()
-    return sorted(set(re.findall(r"\b(efwi_[a-z_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(efwi_[a-z0-9_]+)\s*\(", txt)))
 
 
 def test_library_exports_every_declared_symbol():
