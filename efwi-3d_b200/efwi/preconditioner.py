@@ -227,12 +227,16 @@ class LbfgsResult:
 
 def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10,
           net=None, first_step: float = 20.0, c1: float = 1e-4, max_trials: int = 12,
+          max_expand: int = 3, learned_trials: int = 4,
           stop_misfit: Optional[float] = None, bounds=(1000.0, 6000.0), log=None) -> LbfgsResult:
-    """L-BFGS on vp with a backtracking Armijo line search (trial points
-    cost a forward modelling, the accepted point a gradient).  With `net`,
+    """L-BFGS on vp with an Armijo line search -- backtracking by halves, or
+    doubling (up to max_expand times) while the misfit keeps falling when
+    the unit step is accepted at once; trial points cost a forward
+    modelling, the accepted point a gradient.  With `net`,
     each iteration first tries the CNN's direction (scaled so that its
-    largest vp change is the previous accepted step's); the plain L-BFGS
-    direction is the fallback when that line search fails.  `first_step`
+    largest vp change is the previous accepted step's, at most
+    `learned_trials` halvings); the plain L-BFGS direction is the fallback
+    when that line search fails.  `first_step`
     (m/s) scales the first plain step, like the reference's Adam learning
     rate of 20 m/s (3D_inversion_adam.py)."""
     torch.cuda.synchronize(obj.dev)
@@ -262,15 +266,23 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
             r += s * (a - b)
         return -r
 
-    def search(d, J, g):
+    def search(d, J, g, trials):
         gd = float(torch.sum(g * d))
         if not gd < 0:
             return None
         alpha = 1.0
-        for _ in range(max_trials):
+        for _ in range(trials):
             vn = torch.clamp(vp + alpha * d, *bounds)
             Jn = obj.value(vn)  # trial points need the misfit only
             if Jn <= J + c1 * alpha * gd:
+                if alpha == 1.0:
+                    # accepted at once: extrapolate while the misfit keeps falling
+                    for _ in range(max_expand):
+                        vx = torch.clamp(vp + 2.0 * alpha * d, *bounds)
+                        Jx = obj.value(vx)
+                        if not (Jx < Jn and Jx <= J + c1 * 2.0 * alpha * gd):
+                            break
+                        alpha, vn, Jn = 2.0 * alpha, vx, Jx
                 Jn, gn = obj.value_and_grad(vn)
                 return vn, Jn, gn
             alpha *= 0.5
@@ -282,11 +294,11 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
             with torch.no_grad():
                 dl = -net(features(g, vp, illum))
             dl = dl * (last_dmax / (dl.abs().max() + 1e-30))
-            step = search(dl, J, g)
+            step = search(dl, J, g, learned_trials)
             if step is not None:
                 res.learned_accepted += 1
         if step is None:
-            step = search(two_loop(g), J, g)
+            step = search(two_loop(g), J, g, max_trials)
         if step is None:
             break
         vn, Jn, gn = step
