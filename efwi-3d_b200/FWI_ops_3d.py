@@ -137,6 +137,39 @@ def _shards(ids: List[int], ngpu: int) -> List[List[int]]:
     return [ids[cut[i]:cut[i + 1]] for i in range(ngpu)]
 
 
+class _scratch:
+    """scratch_dir_name (Parameter.cpp:118-124): after the misfit, writes
+    Residual_Shot_{x,y,z}{id}.bin, Syn_Shot_... and CondObs_Shot_... --
+    the adjoint source, the windowed synthetics and the windowed observed
+    data, [nrec][nt] float32 per component (libCUFD.cu:660-700)."""
+
+    def __init__(self, s, ids, obs):
+        self.s, self.ids, self.obs = s, ids, obs
+        self.on = bool(s.para.scratch_dir_name)
+
+    def __enter__(self):
+        if self.on:
+            self.bufs = [torch.empty_like(self.obs) for _ in range(3)]
+            self.s.prop.set_scratch(*self.bufs)
+        return self
+
+    def __exit__(self, et, ev, tb):
+        if not self.on:
+            return False
+        self.s.prop.set_scratch()
+        if et is not None:
+            return False
+        d = self.s.para.scratch_dir_name
+        os.makedirs(d, exist_ok=True)
+        syn, cobs, res = (self.s.prop.split(b.cpu(), self.ids) for b in self.bufs)
+        for k, sid in enumerate(self.ids):
+            for c, name in enumerate("xyz"):
+                for prefix, arr in (("Residual", res), ("Syn", syn), ("CondObs", cobs)):
+                    arr[k][c].numpy().astype(np.float32).tofile(
+                        os.path.join(d, f"{prefix}_Shot_{name}{sid}.bin"))
+        return False
+
+
 def _ids_list(shot_ids) -> List[int]:
     return [int(v) for v in torch.as_tensor(shot_ids).reshape(-1).tolist()]
 
@@ -151,7 +184,9 @@ class _FwiOps:
             s.refresh(stf)
             s.check_ids(ids)
             s.prop.set_model(Lambda, Mu, Den)
-            J = s.prop.misfit(ids, s.observed(ids))
+            obs = s.observed(ids)
+            with _scratch(s, ids, obs):
+                J = s.prop.misfit(ids, obs)
         return [torch.tensor([J], dtype=torch.float32)]
 
     def backward(self, Lambda, Mu, Den, stf, ngpu, shot_ids, para_fname):
@@ -176,7 +211,8 @@ class _FwiOps:
                         n0 = 3 * s.shots[shards[i][0]].nrec * s.para.grid.nt
                         autotune(s.prop, shards[i][0], obs[:n0])
                         s.tuned = True
-                    results[i] = s.prop.gradient(shards[i], obs)
+                    with _scratch(s, shards[i], obs):
+                        results[i] = s.prop.gradient(shards[i], obs)
                     torch.cuda.current_stream(i).synchronize()
             except BaseException as e:  # re-raised on the caller's thread
                 errors[i] = e

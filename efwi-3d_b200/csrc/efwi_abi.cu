@@ -114,6 +114,9 @@ struct EfwiHandle {
   cudaStream_t cap_stream = nullptr;
   long long ck_budget = 4LL << 30;  // bytes of checkpoint slots
   long long ck_forward_steps = 0;   // forward steps of the last exact gradient
+  // optional outputs of the misfit: windowed synthetics / observed data
+  float *scr_syn = nullptr, *scr_obs = nullptr, *scr_res = nullptr;
+  DevBuf scr_tm;
   int ck_slots = 0;                 // slots it used
 
   int prof_sample = 0;
@@ -546,8 +549,10 @@ int resolve_profile(EfwiHandle *h) {
 }
 
 // Misfit of one shot: fills res_tm and adds the sum of squares to *jdev.
+// With efwi_set_scratch outputs set, also writes the windowed synthetics
+// and observed data of the shot at traces offset `off`.
 int misfit_shot(EfwiHandle *h, const ShotHost &sh, const float *obs, const float *syn_tm,
-                float *res_tm, double *jdev, cudaStream_t st) {
+                float *res_tm, double *jdev, cudaStream_t st, long long off) {
   const int nt = h->grid.nt, nr = sh.nrec;
   if (nr == 0) return EFWI_OK;
   dim3 grid((nt + 31) / 32, (nr + 31) / 32, 3);
@@ -563,11 +568,21 @@ int misfit_shot(EfwiHandle *h, const ShotHost &sh, const float *obs, const float
     CK_CUDA(h, cudaMemcpyAsync(w + 2 * nr, sh.wts.data(), sizeof(float) * nr, cudaMemcpyHostToDevice, st));
     m.win_start = w; m.win_end = w + nr; m.weights = w + 2 * nr;
   }
+  const long long ntr = 3LL * nr * nt;
+  if (h->scr_syn || h->scr_obs) {
+    CK_CUDA(h, h->scr_tm.ensure(sizeof(float) * 2 * ntr));
+    m.syn_w = h->scr_tm.as<float>();
+    m.obs_w = m.syn_w + ntr;
+  }
   {
     Timer t(h, K_MISFIT, st, 0);
     k_misfit<<<grid, dim3(32, 8), 0, st>>>(m, obs, syn_tm, res_tm, h->partial.as<double>());
     k_reduce_sum<<<1, 256, 0, st>>>(h->partial.as<double>(), nb, jdev);
   }
+  const dim3 tg((nt + 31) / 32, (nr + 31) / 32, 3);
+  if (h->scr_syn) k_traces_to_cr_t<<<tg, dim3(32, 8), 0, st>>>(m.syn_w, h->scr_syn + off, nt, nr);
+  if (h->scr_obs) k_traces_to_cr_t<<<tg, dim3(32, 8), 0, st>>>(m.obs_w, h->scr_obs + off, nt, nr);
+  if (h->scr_res) k_traces_to_cr_t<<<tg, dim3(32, 8), 0, st>>>(res_tm, h->scr_res + off, nt, nr);
   return check_launch(h, "misfit");
 }
 
@@ -614,7 +629,8 @@ ExactArgs exact_args(EfwiHandle *h, const Fields &f, const Psi &ps, const Fields
 // respect to the traces, traces layout): no misfit is formed and the source
 // is injected as it is, so the images are J^T applied to it.
 int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res_out,
-               float *glam, float *gmu, float *gB, cudaStream_t st, bool adj_source = false) {
+               float *glam, float *gmu, float *gB, cudaStream_t st, bool adj_source = false,
+               long long scratch_off = 0) {
   const int nt = h->grid.nt;
   const int ntl = nt_eff(h);
   const long long N = h->N;
@@ -690,7 +706,8 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
       }
       if (first) {
         first = false;
-        rc = misfit_shot(h, sh, obs, h->traces_tm.as<float>(), h->res_tm.as<float>(), jdev, st);
+        rc = misfit_shot(h, sh, obs, h->traces_tm.as<float>(), h->res_tm.as<float>(), jdev, st,
+                         scratch_off);
         if (rc) return rc;
         if (res_out && sh.nrec > 0) {
           k_traces_to_cr_t<<<dim3((nt + 31) / 32, (sh.nrec + 31) / 32, 3), dim3(32, 8), 0, st>>>(
@@ -808,8 +825,8 @@ int efwi_set_options(EfwiHandle *h, int if_win, int tile_bx, int zchunk, int max
 
 int efwi_set_tuning(EfwiHandle *h, int fwd_cfg, int zchunk_fwd, int rev_cfg, int zchunk_rev) {
   if (!h) return EFWI_ERR_ARG;
-  if (fwd_cfg < 0 || fwd_cfg > 3 || rev_cfg < 0 || rev_cfg > 3 || zchunk_fwd < 0 || zchunk_rev < 0)
-    return fail(h, EFWI_ERR_ARG, "invalid tuning (cfg 0-3, zchunk >= 0)");
+  if (fwd_cfg < 0 || fwd_cfg > 3 || rev_cfg < 0 || rev_cfg > 7 || zchunk_fwd < 0 || zchunk_rev < 0)
+    return fail(h, EFWI_ERR_ARG, "invalid tuning (forward cfg 0-3, reverse cfg 0-7, zchunk >= 0)");
   h->fcfg = fwd_cfg;
   h->rcfg = rev_cfg;
   if (zchunk_fwd) h->zchunk = zchunk_fwd;
@@ -973,7 +990,7 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     for (int k = 0; k < n; ++k) {
       const ShotHost &sh = h->shots[ids[k]];
       int rc = exact_shot(h, ids[k], obs + obs_off, jdev + k, res_out ? res_out + obs_off : nullptr,
-                          glam, gmu, grho, st, adj_source);
+                          glam, gmu, grho, st, adj_source, obs_off);
       if (rc) return rc;
       obs_off += 3LL * sh.nrec * nt;
     }
@@ -992,7 +1009,8 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     int rc = run_forward_batch(h, ids + k, 1, h->traces_tm.as<float>(), ntr, &rec,
                                grad ? h->shell.as<float>() : nullptr, st);
     if (rc) return rc;
-    rc = misfit_shot(h, sh, obs + obs_off, h->traces_tm.as<float>(), h->res_tm.as<float>(), jdev + k, st);
+    rc = misfit_shot(h, sh, obs + obs_off, h->traces_tm.as<float>(), h->res_tm.as<float>(), jdev + k, st,
+                     obs_off);
     if (rc) return rc;
     if (res_out && sh.nrec > 0) {
       k_traces_to_cr_t<<<dim3((nt + 31) / 32, (sh.nrec + 31) / 32, 3), dim3(32, 8), 0, st>>>(
@@ -1015,6 +1033,9 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     // Reverse kernels: TMA-staged (tile 32 x 4) or L1-served.
     Maps<21> m1;
     Maps<23> m2;
+    Maps<13> m1r;
+    Maps<12> m1a;
+    const bool split = h->rcfg >= 6;
     const bool tma = h->variant == 1;
     const EfwiGrid &G = h->grid;
     if (tma) {
@@ -1027,6 +1048,14 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
                              h->buoy.as<float>(), glam, gmu};
       for (int k2 = 0; k2 < 21 && rc == 0; ++k2)
         rc = make_map(h, &m1.m[k2], k2 < 11 ? h1[k2] : p1[k2 - 11], 1, k2 < 11, 4);
+      if (split) {
+        const float *r1[13] = {f.sxz, f.syz, f.sxx, f.sxy, f.syy, f.vz, f.vx, f.vy,
+                               a.vz, a.vx, a.vy, h->buoy.as<float>(), grho};
+        const float *a1[12] = {a.sxz, a.syz, a.sxx, a.sxy, a.syy, a.szz, a.vz, a.vx, a.vy,
+                               h->buoy.as<float>(), h->lam.as<float>(), h->mu.as<float>()};
+        for (int k2 = 0; k2 < 13 && rc == 0; ++k2) rc = make_map(h, &m1r.m[k2], r1[k2], 1, k2 < 5, 4);
+        for (int k2 = 0; k2 < 12 && rc == 0; ++k2) rc = make_map(h, &m1a.m[k2], a1[k2], 1, k2 < 6, 4);
+      }
       for (int k2 = 0; k2 < 23 && rc == 0; ++k2)
         rc = make_map(h, &m2.m[k2], k2 < 6 ? h2[k2] : p2[k2 - 6], 1, k2 < 6, 4);
       if (rc) return rc;
@@ -1039,7 +1068,10 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     int *status = h->status.as<int>();
     auto K1 = [&](int rev, int adj, int it) {
       Timer t(h, K_REV_VELOCITY, st, it);
-      if (tma)
+      if (tma && split)
+        launch_rev_velocity_split_tma(h->rcfg, grid, st, m1r, m1a, h->geo, f, a, ps, grho, zcr,
+                                      nzc, rev, adj, status);
+      else if (tma)
         launch_rev_velocity_tma(h->rcfg, grid, st, m1, h->geo, f, a, ps, grho, zcr, nzc, rev, adj,
                                 status);
       else
@@ -1341,6 +1373,14 @@ int efwi_illumination(EfwiHandle *h, int n, const int *ids, float *h_lam, float 
   rc = check_launch(h, "illumination");
   if (rc) return rc;
   return status_check(h, st);
+}
+
+int efwi_set_scratch(EfwiHandle *h, float *syn_w, float *obs_w, float *res) {
+  if (!h) return EFWI_ERR_ARG;
+  h->scr_syn = syn_w;
+  h->scr_obs = obs_w;
+  h->scr_res = res;
+  return EFWI_OK;
 }
 
 int efwi_set_checkpoint_budget(EfwiHandle *h, long long bytes) {

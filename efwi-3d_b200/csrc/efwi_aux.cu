@@ -146,7 +146,10 @@ k_misfit(MisfitArgs m, const float *obs, const float *syn_tm, float *res_tm, dou
       const float ow = so[rl][tl] * mult, sw = ss[tl][rl] * mult;
       const float rr = (t == 0) ? 0.0f : ow - sw;
       acc += (double)rr * (double)rr;
-      res_tm[((long long)t * 3 + c) * nr + r] = rr * mult;
+      const long long o = ((long long)t * 3 + c) * nr + r;
+      res_tm[o] = rr * mult;
+      if (m.syn_w) m.syn_w[o] = sw;
+      if (m.obs_w) m.obs_w[o] = ow;
     }
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);

@@ -94,6 +94,14 @@ void launch_rev_velocity_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<21>
                              const Geo &g, const Fields &f, const Fields &a, const Psi &ps,
                              float *grho, int zchunk, int nzc, int do_rev, int do_adj,
                              int *status);
+// K1 as two launches (cfg 6, 7): reverse half maps halo sxz syz sxx sxy syy |
+// point vz vx vy avz avx avy | model buoyancy rho-image; adjoint half maps
+// halo asxz asyz asxx asxy asyy aszz | point avz avx avy | model buoyancy
+// lambda mu.
+void launch_rev_velocity_split_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<13> &rev_maps,
+                                   const Maps<12> &adj_maps, const Geo &g, const Fields &f,
+                                   const Fields &a, const Psi &ps, float *grho, int zchunk,
+                                   int nzc, int do_rev, int do_adj, int *status);
 // K2 maps: halo vz vx vy avz avx avy | point szz sxx syy sxz sxy syz aszz
 //          asxx asyy asxz asxy asyz | model lambda mu buoyancy glam gmu.
 void launch_rev_stress_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<23> &maps,
@@ -118,6 +126,7 @@ struct MisfitArgs {
   int if_win;
   const float *win_start, *win_end, *weights;  // [nrec] (if_win)
   float src_weight;
+  float *syn_w, *obs_w;  // optional [nt][3][nrec]: windowed synthetics and observed data
 };
 // obs [3][nrec][nt], syn_tm [nt][3][nrec] -> res_tm [nt][3][nrec];
 // per-CTA partial sums of squares (double) in partial[].

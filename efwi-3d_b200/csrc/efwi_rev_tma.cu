@@ -62,11 +62,29 @@ struct Q4 {
 
 }  // namespace
 
-template <int TX, int R, int MINB>
+// Box layout of K1 by MODE: 0 = reverse velocity + adjoint velocity fused;
+// 1 = reverse velocity + rho image only; 2 = adjoint velocity only (the
+// two halves of mode 0 as separate launches, run 1 then 2).
+template <int MODE>
+struct K1L {
+  static constexpr bool REV = MODE != 2, ADJ = MODE != 1;
+  static constexpr int NH = MODE == 0 ? 11 : (MODE == 1 ? 5 : 6);
+  static constexpr int NPF = MODE == 2 ? 3 : 6;  // field point boxes
+  static constexpr int NM = MODE == 0 ? 4 : (MODE == 1 ? 2 : 3);
+  static constexpr int NP = NPF + NM;
+  static constexpr int N = NH + NP;
+  static constexpr int HA = MODE == 2 ? 0 : 5;  // first adjoint-stress halo box
+  static constexpr int PA = MODE == 2 ? 0 : 3;  // first adjoint-velocity point box
+  static constexpr int MB = NPF, ML = NPF + 1, MM = NPF + 2;  // buoyancy, lambda, mu
+  static constexpr int MG = MODE == 0 ? NPF + 3 : NPF + 1;     // rho image
+};
+
+template <int TX, int R, int MINB, int MODE>
 __global__ void __launch_bounds__(32 * TX, MINB)
-k_rev_velocity_tma(const __grid_constant__ Maps<21> maps, Geo g, Fields f, Fields a, Psi ps,
-                   float *grho, int zchunk, int nzc, int do_rev, int do_adj, int *status) {
-  using Ring = PlaneRing<11, 10, 4, TX, R>;
+k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Fields f, Fields a,
+                   Psi ps, float *grho, int zchunk, int nzc, int do_rev, int do_adj, int *status) {
+  using L = K1L<MODE>;
+  using Ring = PlaneRing<L::NH, L::NP, L::NM, TX, R>;
   extern __shared__ __align__(128) unsigned char smem[];
   Ring ring;
   ring.bind(smem);
@@ -97,10 +115,12 @@ k_rev_velocity_tma(const __grid_constant__ Maps<21> maps, Geo g, Fields f, Field
 
   int i = act ? (int)cell(g, z0, x, y) : 0;
   Q4 szz{}, sxz{}, syz{}, aszz{}, asxx{}, asyy{}, asxz{}, asyz{};
-  if (act) {
+  if (act && L::REV) {
     szz = {f.szz[i - sz], f.szz[i], f.szz[i + sz], f.szz[i + 2 * sz]};
     sxz = {f.sxz[i - 2 * sz], f.sxz[i - sz], f.sxz[i], f.sxz[i + sz]};
     syz = {f.syz[i - 2 * sz], f.syz[i - sz], f.syz[i], f.syz[i + sz]};
+  }
+  if (act && L::ADJ) {
     aszz = {a.szz[i - sz], a.szz[i], a.szz[i + sz], a.szz[i + 2 * sz]};
     asxx = {a.sxx[i - sz], a.sxx[i], a.sxx[i + sz], a.sxx[i + 2 * sz]};
     asyy = {a.syy[i - sz], a.syy[i], a.syy[i + sz], a.syy[i + 2 * sz]};
@@ -114,21 +134,20 @@ k_rev_velocity_tma(const __grid_constant__ Maps<21> maps, Geo g, Fields f, Field
     const int z = z0 + q;
     float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f;
     if (act && q + 1 < nq) {
-      h0 = f.szz[i + 3 * sz]; h1 = f.sxz[i + 2 * sz]; h2 = f.syz[i + 2 * sz];
-      h3 = a.szz[i + 3 * sz]; h4 = a.sxx[i + 3 * sz]; h5 = a.syy[i + 3 * sz];
-      h6 = a.sxz[i + 2 * sz]; h7 = a.syz[i + 2 * sz];
+      if (L::REV) { h0 = f.szz[i + 3 * sz]; h1 = f.sxz[i + 2 * sz]; h2 = f.syz[i + 2 * sz]; }
+      if (L::ADJ) {
+        h3 = a.szz[i + 3 * sz]; h4 = a.sxx[i + 3 * sz]; h5 = a.syy[i + 3 * sz];
+        h6 = a.sxz[i + 2 * sz]; h7 = a.syz[i + 2 * sz];
+      }
     }
     const bool got = ring.wait(q);
     if (act && got) {
-      const BoxView bsxz{ring.halo(q, 0) + off}, bsyz{ring.halo(q, 1) + off},
-          bsxx{ring.halo(q, 2) + off}, bsxy{ring.halo(q, 3) + off}, bsyy{ring.halo(q, 4) + off};
-      const BoxView basxz{ring.halo(q, 5) + off}, basyz{ring.halo(q, 6) + off},
-          basxx{ring.halo(q, 7) + off}, basxy{ring.halo(q, 8) + off},
-          basyy{ring.halo(q, 9) + off}, baszz{ring.halo(q, 10) + off};
-      const float b = ring.point(q, 6)[pt];
-      const float avz0 = ring.point(q, 3)[pt], avx0 = ring.point(q, 4)[pt],
-                  avy0 = ring.point(q, 5)[pt];
-      if (do_rev && xin && yin && z >= np && z <= nz - 1 - np) {
+      const float b = ring.point(q, L::MB)[pt];
+      const float avz0 = ring.point(q, L::PA)[pt], avx0 = ring.point(q, L::PA + 1)[pt],
+                  avy0 = ring.point(q, L::PA + 2)[pt];
+      if (L::REV && do_rev && xin && yin && z >= np && z <= nz - 1 - np) {
+        const BoxView bsxz{ring.halo(q, 0) + off}, bsyz{ring.halo(q, 1) + off},
+            bsxx{ring.halo(q, 2) + off}, bsxy{ring.halo(q, 3) + off}, bsyy{ring.halo(q, 4) + off};
         const float sxy_0 = bsxy.c(), sxy_xm1 = bsxy.x(-1);
         const float dz_ = dplus(szz.a, szz.b, szz.c, szz.d) * idz +
                           dminus(bsxz.x(-2), bsxz.x(-1), sxz.c, bsxz.x(1)) * idx +
@@ -143,13 +162,16 @@ k_rev_velocity_tma(const __grid_constant__ Maps<21> maps, Geo g, Fields f, Field
         f.vx[i] = ring.point(q, 1)[pt] - dx_ * b * dt;
         f.vy[i] = ring.point(q, 2)[pt] - dy_ * b * dt;
         const float nb2 = -(b * b);
-        grho[i] = ring.point(q, 9)[pt] -
+        grho[i] = ring.point(q, L::MG)[pt] -
                     (avz0 * dz_ * dt * nb2 + avx0 * dx_ * dt * nb2 + avy0 * dy_ * dt * nb2);
       }
-      if (do_adj) {
+      if (L::ADJ && do_adj) {
+        const BoxView basxz{ring.halo(q, L::HA) + off}, basyz{ring.halo(q, L::HA + 1) + off},
+            basxx{ring.halo(q, L::HA + 2) + off}, basxy{ring.halo(q, L::HA + 3) + off},
+            basyy{ring.halo(q, L::HA + 4) + off}, baszz{ring.halo(q, L::HA + 5) + off};
         const bool zs = slab_s(z, nz, np);
         const Coef cz = coef(g.cz, nz, z);
-        const float l = ring.point(q, 7)[pt], u = ring.point(q, 8)[pt], l2u = l + 2.0f * u;
+        const float l = ring.point(q, L::ML)[pt], u = ring.point(q, L::MM)[pt], l2u = l + 2.0f * u;
         {  // adjoint vx
           const float dszz_dx = -dplus(baszz.x(-1), aszz.b, baszz.x(1), baszz.x(2)) * idx;
           const float dsxx_dx = -dplus(basxx.x(-1), asxx.b, basxx.x(1), basxx.x(2)) * idx;
@@ -393,15 +415,16 @@ void set_smem(K kernel, int bytes) {
 
 // Launch configurations of the reverse TMA kernels (32 x 4 tiles):
 // (ring depth, minimum resident CTAs per SM).
-template <int R, int MINB>
-static void revv_launch(dim3 grid, cudaStream_t st, const Maps<21> &maps, const Geo &g,
+template <int R, int MINB, int MODE = 0>
+static void revv_launch(dim3 grid, cudaStream_t st, const Maps<K1L<MODE>::N> &maps, const Geo &g,
                         const Fields &f, const Fields &a, const Psi &ps, float *grho, int zchunk,
                         int nzc, int do_rev, int do_adj, int *status) {
-  constexpr int B = PlaneRing<11, 10, 4, 4, R>::BYTES;
-  static bool once = (set_smem(k_rev_velocity_tma<4, R, MINB>, B), true);
+  using L = K1L<MODE>;
+  constexpr int B = PlaneRing<L::NH, L::NP, L::NM, 4, R>::BYTES;
+  static bool once = (set_smem(k_rev_velocity_tma<4, R, MINB, MODE>, B), true);
   (void)once;
-  k_rev_velocity_tma<4, R, MINB><<<grid, dim3(32, 4), B, st>>>(maps, g, f, a, ps, grho, zchunk,
-                                                              nzc, do_rev, do_adj, status);
+  k_rev_velocity_tma<4, R, MINB, MODE><<<grid, dim3(32, 4), B, st>>>(
+      maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status);
 }
 
 template <int R, int MINB>
@@ -424,7 +447,24 @@ void launch_rev_velocity_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<21>
     case 1: revv_launch<2, 4>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
     case 2: revv_launch<3, 4>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
     case 3: revv_launch<2, 1>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
+    case 4: revv_launch<2, 5>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
+    case 5: revv_launch<2, 6>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
     default: revv_launch<3, 1>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
+  }
+}
+
+// Split K1 (cfg 6: rings of 2 planes; cfg 7: 3 planes): the reverse
+// velocity half, then the adjoint velocity half.
+void launch_rev_velocity_split_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<13> &rev_maps,
+                                   const Maps<12> &adj_maps, const Geo &g, const Fields &f,
+                                   const Fields &a, const Psi &ps, float *grho, int zchunk,
+                                   int nzc, int do_rev, int do_adj, int *status) {
+  if (cfg == 7) {
+    if (do_rev) revv_launch<3, 8, 1>(grid, st, rev_maps, g, f, a, ps, grho, zchunk, nzc, 1, 0, status);
+    if (do_adj) revv_launch<3, 4, 2>(grid, st, adj_maps, g, f, a, ps, grho, zchunk, nzc, 0, 1, status);
+  } else {
+    if (do_rev) revv_launch<2, 8, 1>(grid, st, rev_maps, g, f, a, ps, grho, zchunk, nzc, 1, 0, status);
+    if (do_adj) revv_launch<2, 5, 2>(grid, st, adj_maps, g, f, a, ps, grho, zchunk, nzc, 0, 1, status);
   }
 }
 
@@ -436,6 +476,10 @@ void launch_rev_stress_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<23> &
     case 1: revs_launch<2, 5>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
     case 2: revs_launch<3, 4>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
     case 3: revs_launch<2, 1>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
+    case 4: revs_launch<2, 6>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
+    case 5: revs_launch<2, 7>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
+    case 6: revs_launch<2, 5>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
+    case 7: revs_launch<3, 4>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
     default: revs_launch<3, 1>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
   }
 }

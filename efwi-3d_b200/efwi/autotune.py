@@ -15,8 +15,8 @@ from typing import Dict, Sequence
 import torch
 
 FWD_CFGS = (0, 1, 2, 3)
-REV_CFGS = (0, 1, 2, 3)
-ZCHUNKS = (4, 8, 12, 16)
+REV_CFGS = (0, 1, 2, 3, 4, 5, 6, 7)
+ZCHUNKS = (2, 3, 4, 6, 8)
 
 
 def _probe(P, shot_ids, obs, names) -> float:

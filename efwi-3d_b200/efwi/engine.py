@@ -232,6 +232,15 @@ class Propagator:
             return J.value, gl, gm, gr, res
         return J.value, gl, gm, gr
 
+    def set_scratch(self, syn_w=None, obs_w=None, res=None) -> None:
+        """Device buffers (traces layout of the next calls' obs) that every
+        misfit also fills with windowed synthetics, windowed observed data
+        and the adjoint source; None disables."""
+        self._scratch = (syn_w, obs_w, res)
+        ptr = [C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+               for t in (syn_w, obs_w, res)]
+        check(self._h, self._L.efwi_set_scratch(self._h, *ptr))
+
     def forward_windows(self, shot_ids, windows, use_graph: bool = True) -> torch.Tensor:
         """Traces of shots each on its own window (x0, y0, nx, ny) of the
         padded grid, all windows in one persistent launch per half-step."""

@@ -76,8 +76,9 @@ int efwi_set_options(EfwiHandle *h, int if_win, int tile_bx, int zchunk, int max
 int efwi_set_variant(EfwiHandle *h, int variant);
 
 /* Launch configuration of the TMA kernels (the autotuner's knobs; results
- * do not depend on them): fwd_cfg / rev_cfg in 0..3 select tile, ring depth
- * and occupancy target; zchunk_* > 0 sets the z planes per CTA (0 keeps).
+ * do not depend on them): fwd_cfg in 0..3 and rev_cfg in 0..7 select tile,
+ * ring depth and occupancy target (rev_cfg 6, 7 run the reverse-velocity
+ * kernel as two launches); zchunk_* > 0 sets the z planes per CTA (0 keeps).
  * No reference counterpart. */
 int efwi_set_tuning(EfwiHandle *h, int fwd_cfg, int zchunk_fwd, int rev_cfg, int zchunk_rev);
 
@@ -177,6 +178,13 @@ int efwi_checkpoint_plan(int nt, int slots, long long *forward_steps, int *slots
  * (full grids; only their C-PML slabs are read and written).  No reference
  * counterpart; it serves dot-product tests of the adjoint. */
 int efwi_step(EfwiHandle *h, float *state, int transpose, void *stream);
+
+/* Scratch outputs (the reference's scratch_dir_name dumps,
+ * libCUFD.cu:660-700): while set, every misfit of efwi_misfit /
+ * efwi_gradient also writes the windowed synthetics (syn_w), the windowed
+ * observed data (obs_w) and the adjoint source (res) of its shots -- device
+ * buffers in the traces layout of that call's `obs`; NULL disables each. */
+int efwi_set_scratch(EfwiHandle *h, float *syn_w, float *obs_w, float *res);
 
 /* Misfit and adjoint source of one shot with no device allocation.  No
  * counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -199,7 +199,8 @@ def test_all_launch_configurations_give_identical_results():
     base.set_tuning(0, 8, 0, 8)
     ref_tr = base.forward([0]).cpu()
     ref_g = base.gradient([0], obs)
-    for fc, zf, rc, zr in [(1, 4, 1, 4), (2, 12, 2, 16), (3, 5, 3, 3), (0, 64, 1, 64)]:
+    for fc, zf, rc, zr in [(1, 4, 1, 4), (2, 12, 2, 16), (3, 5, 3, 3), (0, 64, 1, 64),
+                           (1, 2, 4, 2), (2, 3, 5, 6), (1, 4, 6, 4), (0, 8, 7, 3)]:
         P = _prop("B_")
         P.set_tuning(fc, zf, rc, zr)
         assert torch.equal(P.forward([0]).cpu(), ref_tr)
