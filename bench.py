@@ -58,7 +58,8 @@ def parse():
                     help="profiling case 'gradient' or 'exact': one shot of the grid, --nt "
                          "steps, tuning --tuning, forward of the true model then one gradient")
     ap.add_argument("--tuning", default="1,4,1,4",
-                    help="forward cfg, forward zchunk, reverse cfg, reverse zchunk")
+                    help="forward cfg, forward zchunk, reverse cfg, reverse zchunk (profiling "
+                         "cases, and the main run with --no-autotune)")
     ap.add_argument("--iters", type=int, default=20, help="inversion case: L-BFGS iterations")
     ap.add_argument("--pairs", type=int, default=200, help="inversion case: training pairs")
     ap.add_argument("--pair-n", type=int, default=40, help="inversion case: model cells of a pair")
@@ -449,7 +450,11 @@ def main():
     lam, mu, rho = (torch.from_numpy(x).to(dev) for x in prob.params("init"))
     P.set_model(lam, mu, rho)
     from efwi.autotune import autotune
-    tune = autotune(P, 0, P.split(obs, ids)[0].reshape(-1)) if a.autotune else None
+    if a.autotune:
+        tune = autotune(P, 0, P.split(obs, ids)[0].reshape(-1))
+    else:
+        P.set_tuning(*[int(v) for v in a.tuning.split(",")])
+        tune = {"fixed": a.tuning}
 
     stream = torch.cuda.current_stream(dev)
 

@@ -1274,7 +1274,6 @@ int efwi_forward_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow 
       if (nr > 0) k_record_multi<<<(int)((nr + 127) / 128), 128, 0, s>>>(ddom, drd, drc, drr, (int)nr, ttm, it + 1);
     }
   };
-  const long long per_step = 2 + (nr > 0 ? 1 : 0);
   if (use_graph) {
     if (!h->cap_stream) CK_CUDA(h, cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
     cudaStream_t cs = h->cap_stream;
@@ -1303,7 +1302,6 @@ int efwi_forward_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow 
   h->launches[K_STRESS_FWD] += ntl - 1;
   h->launches[K_VELOCITY_FWD] += ntl - 1;
   if (nr > 0) h->launches[K_RECORD] += ntl - 1;
-  (void)per_step;
   long long off = 0;
   for (int k = 0; k < n; ++k) {
     const int nrs = dom[k].nrec;

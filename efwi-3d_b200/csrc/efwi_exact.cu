@@ -32,9 +32,10 @@
 // (two buffers used in turn): neighbours read them while the owner updates.
 //
 // Tiling: a CTA owns a 32 (y) x BX (x) column tile and marches a chunk of z
-// planes.  The Q of the x- and y-axis terms are staged in shared memory per
-// plane (tile plus a 2-cell halo), those of the z-axis terms in register
-// queues; the forward fields of the images are read through L1.
+// planes.  The Q of the x- and y-axis terms and the forward fields of the
+// images are staged in shared memory per plane (tile plus a 2-cell halo),
+// the z-axis terms in register queues; every global load of a plane is
+// issued before the plane's one barrier.
 #include "efwi_common.cuh"
 #include "efwi_exact.h"
 
@@ -181,6 +182,9 @@ template <int BX>
 __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int zchunk, int nzc) {
   __shared__ float sqx[2][3][BX + 4][32];
   __shared__ float sqy[2][3][BX][36];
+  // forward velocities of the images (vz, vx, vy) along x and along y
+  __shared__ float sfx[2][3][BX + 4][32];
+  __shared__ float sfy[2][3][BX][36];
   const Geo &g = A.g;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int y = blockIdx.x * 32 + tx;
@@ -191,7 +195,6 @@ __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int z
   if (z0 >= z1) return;  // uniform over the CTA
   const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
   const int sz = (int)g.sz;
-  const int sx = g.sx;
   const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
   const bool xin = x >= 2 && x <= nx - 3, yin = y >= 2 && y <= ny - 3;
   const bool act = xin && yin;
@@ -209,6 +212,19 @@ __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int z
     qez[k] = qvx[k] = qvy[k] = 0.f;
     if (act) qs_z(A, z0 - 2 + k, x, y, qez[k], qvx[k], qvy[k]);
   }
+  // z queues of the forward velocities: vz at z-2 .. z+1, vx and vy at z-1 .. z+2
+  const float *fvz = A.f.vz, *fvx = A.f.vx, *fvy = A.f.vy;
+  float zvz[4] = {0.f, 0.f, 0.f, 0.f}, zvx[4] = {0.f, 0.f, 0.f, 0.f}, zvy[4] = {0.f, 0.f, 0.f, 0.f};
+  if (act) {
+    const int i0 = cell32(g, z0, x, y);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      zvz[k] = fvz[i0 + (k - 2) * sz];
+      zvx[k] = fvx[i0 + (k - 1) * sz];
+      zvy[k] = fvy[i0 + (k - 1) * sz];
+    }
+  }
+  const bool hxin = hxn >= 0 && hxn < nx, hyin = hyn >= 0 && hyn < ny;
 
   int buf = 0;
   for (int z = z0; z < z1; ++z, buf ^= 1) {
@@ -217,17 +233,35 @@ __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int z
     float ox[3] = {0.f, 0.f, 0.f}, oy[3] = {0.f, 0.f, 0.f};
     GS G{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (act) G = qs_own(A, z, x, y, ox, oy);
+    float fo[3] = {0.f, 0.f, 0.f};  // own vz vx vy
+    if (act) {
+      const int i = cell32(g, z, x, y);
+      fo[0] = fvz[i]; fo[1] = fvx[i]; fo[2] = fvy[i];
+    }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { sqx[buf][k][ty + 2][tx] = ox[k]; sqy[buf][k][ty][tx + 2] = oy[k]; }
+    for (int k = 0; k < 3; ++k) {
+      sqx[buf][k][ty + 2][tx] = ox[k]; sqy[buf][k][ty][tx + 2] = oy[k];
+      sfx[buf][k][ty + 2][tx] = fo[k]; sfy[buf][k][ty][tx + 2] = fo[k];
+    }
     if (ty < 4) {
-      float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
       if (yin) qs_x(A, z, hxn, y, h0, h1, h2);
+      if (yin && hxin) {
+        const int j = cell32(g, z, hxn, y);
+        f0 = fvz[j]; f1 = fvx[j]; f2 = fvy[j];
+      }
       sqx[buf][0][hr][tx] = h0; sqx[buf][1][hr][tx] = h1; sqx[buf][2][hr][tx] = h2;
+      sfx[buf][0][hr][tx] = f0; sfx[buf][1][hr][tx] = f1; sfx[buf][2][hr][tx] = f2;
     }
     if (tx < 4) {
-      float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
       if (xin) qs_y(A, z, x, hyn, h0, h1, h2);
+      if (xin && hyin) {
+        const int j = cell32(g, z, x, hyn);
+        f0 = fvz[j]; f1 = fvx[j]; f2 = fvy[j];
+      }
       sqy[buf][0][ty][hc] = h0; sqy[buf][1][ty][hc] = h1; sqy[buf][2][ty][hc] = h2;
+      sfy[buf][0][ty][hc] = f0; sfy[buf][1][ty][hc] = f1; sfy[buf][2][ty][hc] = f2;
     }
     __syncthreads();
 
@@ -247,16 +281,17 @@ __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int z
                         dminus(qvy[0], qvy[1], qvy[2], qvy[3]) * idz;
 
       // ---- images from the forward velocities of the same step
-      const float *vz = A.f.vz, *vx = A.f.vx, *vy = A.f.vy;
-      float ezz = dminus(vz[i - 2 * sz], vz[i - sz], vz[i], vz[i + sz]) * idz;
-      float exx = dminus(vx[i - 2 * sx], vx[i - sx], vx[i], vx[i + sx]) * idx;
-      float eyy = dminus(vy[i - 2], vy[i - 1], vy[i], vy[i + 1]) * idy;
-      float dvx_dz = dplus(vx[i - sz], vx[i], vx[i + sz], vx[i + 2 * sz]) * idz;
-      float dvy_dz = dplus(vy[i - sz], vy[i], vy[i + sz], vy[i + 2 * sz]) * idz;
-      float dvx_dy = dplus(vx[i - 1], vx[i], vx[i + 1], vx[i + 2]) * idy;
-      float dvz_dx = dplus(vz[i - sx], vz[i], vz[i + sx], vz[i + 2 * sx]) * idx;
-      float dvz_dy = dplus(vz[i - 1], vz[i], vz[i + 1], vz[i + 2]) * idy;
-      float dvy_dx = dplus(vy[i - sx], vy[i], vy[i + sx], vy[i + 2 * sx]) * idx;
+      const float(*FX)[BX + 4][32] = sfx[buf];
+      const float(*FY)[BX][36] = sfy[buf];
+      float ezz = dminus(zvz[0], zvz[1], zvz[2], zvz[3]) * idz;
+      float exx = dminus(FX[1][ty][tx], FX[1][ty + 1][tx], FX[1][ty + 2][tx], FX[1][ty + 3][tx]) * idx;
+      float eyy = dminus(FY[2][ty][tx], FY[2][ty][tx + 1], FY[2][ty][tx + 2], FY[2][ty][tx + 3]) * idy;
+      float dvx_dz = dplus(zvx[0], zvx[1], zvx[2], zvx[3]) * idz;
+      float dvy_dz = dplus(zvy[0], zvy[1], zvy[2], zvy[3]) * idz;
+      float dvx_dy = dplus(FY[1][ty][tx + 1], FY[1][ty][tx + 2], FY[1][ty][tx + 3], FY[1][ty][tx + 4]) * idy;
+      float dvz_dx = dplus(FX[0][ty + 1][tx], FX[0][ty + 2][tx], FX[0][ty + 3][tx], FX[0][ty + 4][tx]) * idx;
+      float dvz_dy = dplus(FY[0][ty][tx + 1], FY[0][ty][tx + 2], FY[0][ty][tx + 3], FY[0][ty][tx + 4]) * idy;
+      float dvy_dx = dplus(FX[2][ty + 1][tx], FX[2][ty + 2][tx], FX[2][ty + 3][tx], FX[2][ty + 4][tx]) * idx;
       if (slab_s(z, nz, np)) {
         const float *c = g.cz;
         const float Kz = c[CK * nz + z], az = c[CA * nz + z], bz = c[CB * nz + z];
@@ -309,6 +344,14 @@ __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int z
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) { qez[k] = qez[k + 1]; qvx[k] = qvx[k + 1]; qvy[k] = qvy[k + 1]; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { zvz[k] = zvz[k + 1]; zvx[k] = zvx[k + 1]; zvy[k] = zvy[k + 1]; }
+    if (act && z + 1 < z1) {
+      const int i = cell32(g, z, x, y);
+      zvz[3] = fvz[i + 2 * sz];
+      zvx[3] = fvx[i + 3 * sz];
+      zvy[3] = fvy[i + 3 * sz];
+    }
   }
 }
 
@@ -415,6 +458,9 @@ template <int BX>
 __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int zchunk, int nzc) {
   __shared__ float sqx[2][3][BX + 4][32];
   __shared__ float sqy[2][3][BX][36];
+  // forward stresses of the image: sxz, sxx, sxy along x; syz, sxy, syy along y
+  __shared__ float sfx[2][3][BX + 4][32];
+  __shared__ float sfy[2][3][BX][36];
   const Geo &g = A.g;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int y = blockIdx.x * 32 + tx;
@@ -425,7 +471,6 @@ __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int
   if (z0 >= z1) return;  // uniform over the CTA
   const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
   const int sz = (int)g.sz;
-  const int sx = g.sx;
   const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
   const bool xin = x >= 2 && x <= nx - 3, yin = y >= 2 && y <= ny - 3;
   const bool act = xin && yin;
@@ -441,6 +486,20 @@ __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int
     qzz[k] = qxz[k] = qyz[k] = 0.f;
     if (act) qv_z(A, z0 - 2 + k, x, y, qzz[k], qxz[k], qyz[k]);
   }
+  // z queues of the forward stresses: szz at z-1 .. z+2, sxz and syz at z-2 .. z+1
+  const float *fszz = A.f.szz, *fsxx = A.f.sxx, *fsyy = A.f.syy;
+  const float *fsxz = A.f.sxz, *fsxy = A.f.sxy, *fsyz = A.f.syz;
+  float zszz[4] = {0.f, 0.f, 0.f, 0.f}, zsxz[4] = {0.f, 0.f, 0.f, 0.f}, zsyz[4] = {0.f, 0.f, 0.f, 0.f};
+  if (act) {
+    const int i0 = cell32(g, z0, x, y);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      zszz[k] = fszz[i0 + (k - 1) * sz];
+      zsxz[k] = fsxz[i0 + (k - 2) * sz];
+      zsyz[k] = fsyz[i0 + (k - 2) * sz];
+    }
+  }
+  const bool hxin = hxn >= 0 && hxn < nx, hyin = hyn >= 0 && hyn < ny;
 
   int buf = 0;
   for (int z = z0; z < z1; ++z, buf ^= 1) {
@@ -449,17 +508,34 @@ __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int
     float ox[3] = {0.f, 0.f, 0.f}, oy[3] = {0.f, 0.f, 0.f};
     float gz = 0.f, gx = 0.f, gy = 0.f;
     if (act) qv_own(A, z, x, y, gz, gx, gy, ox, oy);
+    float fo[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // own sxz sxx sxy syz syy
+    if (act) {
+      const int i = cell32(g, z, x, y);
+      fo[0] = fsxz[i]; fo[1] = fsxx[i]; fo[2] = fsxy[i]; fo[3] = fsyz[i]; fo[4] = fsyy[i];
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) { sqx[buf][k][ty + 2][tx] = ox[k]; sqy[buf][k][ty][tx + 2] = oy[k]; }
+    sfx[buf][0][ty + 2][tx] = fo[0]; sfx[buf][1][ty + 2][tx] = fo[1]; sfx[buf][2][ty + 2][tx] = fo[2];
+    sfy[buf][0][ty][tx + 2] = fo[3]; sfy[buf][1][ty][tx + 2] = fo[2]; sfy[buf][2][ty][tx + 2] = fo[4];
     if (ty < 4) {
-      float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
       if (yin) qv_x(A, z, hxn, y, h0, h1, h2);
+      if (yin && hxin) {
+        const int j = cell32(g, z, hxn, y);
+        f0 = fsxz[j]; f1 = fsxx[j]; f2 = fsxy[j];
+      }
       sqx[buf][0][hr][tx] = h0; sqx[buf][1][hr][tx] = h1; sqx[buf][2][hr][tx] = h2;
+      sfx[buf][0][hr][tx] = f0; sfx[buf][1][hr][tx] = f1; sfx[buf][2][hr][tx] = f2;
     }
     if (tx < 4) {
-      float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
       if (xin) qv_y(A, z, x, hyn, h0, h1, h2);
+      if (xin && hyin) {
+        const int j = cell32(g, z, x, hyn);
+        f0 = fsyz[j]; f1 = fsxy[j]; f2 = fsyy[j];
+      }
       sqy[buf][0][ty][hc] = h0; sqy[buf][1][ty][hc] = h1; sqy[buf][2][ty][hc] = h2;
+      sfy[buf][0][ty][hc] = f0; sfy[buf][1][ty][hc] = f1; sfy[buf][2][ty][hc] = f2;
     }
     __syncthreads();
 
@@ -480,17 +556,18 @@ __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int
                          dq_t(QX[2][ty + 2][tx], QX[2][ty + 3][tx], QX[2][ty + 4][tx]) * idx;
 
       // ---- buoyancy image from the forward stresses of the same step
-      const float *szz = A.f.szz, *sxx = A.f.sxx, *syy = A.f.syy;
-      const float *sxz = A.f.sxz, *sxy = A.f.sxy, *syz = A.f.syz;
-      float dszz_dz = dplus(szz[i - sz], szz[i], szz[i + sz], szz[i + 2 * sz]) * idz;
-      float dsxz_dx = dminus(sxz[i - 2 * sx], sxz[i - sx], sxz[i], sxz[i + sx]) * idx;
-      float dsyz_dy = dminus(syz[i - 2], syz[i - 1], syz[i], syz[i + 1]) * idy;
-      float dsxz_dz = dminus(sxz[i - 2 * sz], sxz[i - sz], sxz[i], sxz[i + sz]) * idz;
-      float dsxx_dx = dplus(sxx[i - sx], sxx[i], sxx[i + sx], sxx[i + 2 * sx]) * idx;
-      float dsxy_dy = dminus(sxy[i - 2], sxy[i - 1], sxy[i], sxy[i + 1]) * idy;
-      float dsyz_dz = dminus(syz[i - 2 * sz], syz[i - sz], syz[i], syz[i + sz]) * idz;
-      float dsxy_dx = (EFWI_C1 * (sxy[i] - sxy[i - sx]) - EFWI_C2 * (sxy[i - sx] - sxy[i - 2 * sx])) * idx;
-      float dsyy_dy = dplus(syy[i - 1], syy[i], syy[i + 1], syy[i + 2]) * idy;
+      const float(*FX)[BX + 4][32] = sfx[buf];
+      const float(*FY)[BX][36] = sfy[buf];
+      float dszz_dz = dplus(zszz[0], zszz[1], zszz[2], zszz[3]) * idz;
+      float dsxz_dx = dminus(FX[0][ty][tx], FX[0][ty + 1][tx], FX[0][ty + 2][tx], FX[0][ty + 3][tx]) * idx;
+      float dsyz_dy = dminus(FY[0][ty][tx], FY[0][ty][tx + 1], FY[0][ty][tx + 2], FY[0][ty][tx + 3]) * idy;
+      float dsxz_dz = dminus(zsxz[0], zsxz[1], zsxz[2], zsxz[3]) * idz;
+      float dsxx_dx = dplus(FX[1][ty + 1][tx], FX[1][ty + 2][tx], FX[1][ty + 3][tx], FX[1][ty + 4][tx]) * idx;
+      float dsxy_dy = dminus(FY[1][ty][tx], FY[1][ty][tx + 1], FY[1][ty][tx + 2], FY[1][ty][tx + 3]) * idy;
+      float dsyz_dz = dminus(zsyz[0], zsyz[1], zsyz[2], zsyz[3]) * idz;
+      const float sxy0 = FX[2][ty + 2][tx], sxym1 = FX[2][ty + 1][tx], sxym2 = FX[2][ty][tx];
+      float dsxy_dx = (EFWI_C1 * (sxy0 - sxym1) - EFWI_C2 * (sxym1 - sxym2)) * idx;
+      float dsyy_dy = dplus(FY[2][ty][tx + 1], FY[2][ty][tx + 2], FY[2][ty][tx + 3], FY[2][ty][tx + 4]) * idy;
       if (slab_s(z, nz, np)) {
         const float *c = g.cz;
         const float Kz = c[CK * nz + z], bz = c[CB * nz + z], Kzh = c[CKH * nz + z], bzh = c[CBH * nz + z];
@@ -540,6 +617,14 @@ __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) { qzz[k] = qzz[k + 1]; qxz[k] = qxz[k + 1]; qyz[k] = qyz[k + 1]; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { zszz[k] = zszz[k + 1]; zsxz[k] = zsxz[k + 1]; zsyz[k] = zsyz[k + 1]; }
+    if (act && z + 1 < z1) {
+      const int i = cell32(g, z, x, y);
+      zszz[3] = fszz[i + 3 * sz];
+      zsxz[3] = fsxz[i + 2 * sz];
+      zsyz[3] = fsyz[i + 2 * sz];
+    }
   }
 }
 

@@ -128,13 +128,15 @@ class VpObjective:
         return float(self.P.misfit(self.ids, self.obs))
 
     def _to_vp(self, vp: torch.Tensor, g_lam: torch.Tensor, square: bool = False) -> torch.Tensor:
-        """Chain a lambda-space quantity to vp (dlambda/dvp = 2 vp rho)."""
-        v = vp.detach().clone().requires_grad_(True)
-        lam, _, _ = self.params(v)
+        """Chain a lambda-space quantity to vp (dlambda/dvp = 2 vp rho): a
+        gradient through the padding, or (square) a diagonal on the model
+        grid."""
         if square:
             d = 2.0 * self._pad(vp) * self.rho_p
             p = self.npml
             return (g_lam * d * d)[p:-p, p:-p, p:-p]
+        v = vp.detach().clone().requires_grad_(True)
+        lam, _, _ = self.params(v)
         (g,) = torch.autograd.grad(lam, v, grad_outputs=g_lam)
         return g
 
