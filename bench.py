@@ -267,7 +267,7 @@ def run_case(a):
     from efwi import synthetic
     from efwi.engine import Propagator
     p = synthetic.config2(nt=a.nt, nshot=1, n=a.n)
-    P = Propagator(p.grid)
+    P = Propagator(p.grid, tile_bx=a.tile_bx)
     P.set_tuning(*[int(v) for v in a.tuning.split(",")])
     P.set_survey(p.shots, p.stf)
     P.set_model(*[torch.from_numpy(x) for x in p.params("true")])
@@ -405,8 +405,51 @@ def run_windows(a):
     P.close()
 
 
+def run_cnn(a):
+    """The preconditioner CNN (4 BF16 tensor-core 3x3x3 convolutions, 16
+    channels) on one a.n^3 volume: forward, and forward + backward, timed
+    with CUDA events; FLOPs counted as 2*27*16*16 per voxel and layer
+    (the input gradient and the weight gradient add two more convolutions
+    per layer in the backward pass)."""
+    import torch
+    from efwi.cnn import Preconditioner
+    torch.cuda.set_device(0)
+    net = Preconditioner(cin=3, seed=0).cuda()
+    feats = torch.randn(3, a.n, a.n, a.n, device="cuda")
+    vox = a.n ** 3
+    layers = len(net.w)
+    for _ in range(3):
+        net(feats).sum().backward()
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
+    for _ in range(a.steps):
+        with torch.no_grad():
+            net(feats)
+    e[1].record()
+    e[2].record()
+    for _ in range(a.steps):
+        net(feats).sum().backward()
+    e[3].record()
+    torch.cuda.synchronize()
+    fwd_ms = e[0].elapsed_time(e[1]) / a.steps
+    all_ms = e[2].elapsed_time(e[3]) / a.steps
+    fl = 2.0 * 27 * 16 * 16 * vox * layers
+    d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = float(d.get("bf16_tflops", 1590.0))
+    print(json.dumps({"case": "cnn", "grid": a.n, "layers": layers, "fwd_ms": fwd_ms,
+                      "fwd_bwd_ms": all_ms, "fwd_tflops": fl / (fwd_ms * 1e-3) / 1e12,
+                      "fwd_bwd_tflops": 3 * fl / (all_ms * 1e-3) / 1e12,
+                      "peak_bf16_tflops": peak,
+                      "note": "mma.sync m16n8k16 BF16 kernels, FP32 accumulation"}))
+
+
 def main():
     a = parse()
+    if a.case == "cnn":
+        run_cnn(a)
+        return
     if a.case == "inversion":
         run_inversion(a)
         return

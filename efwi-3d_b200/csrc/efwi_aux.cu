@@ -143,7 +143,9 @@ k_misfit(MisfitArgs m, const float *obs, const float *syn_tm, float *res_tm, dou
     const int t = t0 + tl, r = r0 + rl;
     if (t < nt && r < nr) {
       const float mult = window_mult(m, t, r);
-      const float ow = so[rl][tl] * mult, sw = ss[tl][rl] * mult;
+      // windowed traces rounded on their own, as the reference windows the
+      // data in place before subtracting (cuda_window, then gpuMinus)
+      const float ow = __fmul_rn(so[rl][tl], mult), sw = __fmul_rn(ss[tl][rl], mult);
       const float rr = (t == 0) ? 0.0f : ow - sw;
       acc += (double)rr * (double)rr;
       const long long o = ((long long)t * 3 + c) * nr + r;

@@ -54,7 +54,7 @@ k_misfit_direct(MisfitArgs m, const float *obs, const float *syn, float *res, do
     if (t < nt && r < nr) {
       const long long i = ((long long)c * nr + r) * nt + t;
       const float mult = window_mult(m, t, r);
-      const float ow = obs[i] * mult, sw = syn[i] * mult;
+      const float ow = __fmul_rn(obs[i], mult), sw = __fmul_rn(syn[i], mult);
       const float rr = (t == 0) ? 0.0f : ow - sw;
       acc += (double)rr * (double)rr;
       res[i] = rr * mult;
