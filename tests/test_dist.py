@@ -2,9 +2,6 @@
 on the CPU: the shards cover the shot list once, in order, by the
 reference's linspace rule (Torch_Fwi.cpp:53-54), and after the all-reduce
 every rank holds the sum over all shots."""
-import os
-import socket
-
 import pytest
 import torch
 import torch.distributed as dist
@@ -40,11 +37,11 @@ class FakeProp:
         return J, gl, gm, gr
 
 
-def _worker(rank, world, port, ids, q):
-    os.environ["MASTER_ADDR"] = "127.0.0.1"
-    os.environ["MASTER_PORT"] = str(port)
+def _worker(rank, world, store_path, ids, q):
     from datetime import timedelta
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    # file rendezvous: no TCP port to collide with other processes
+    dist.init_process_group("gloo", init_method=f"file://{store_path}", rank=rank,
+                            world_size=world, timeout=timedelta(seconds=60))
     try:
         sp = edist.ShotParallel(FakeProp())
         mine = sp.local_ids(ids)
@@ -54,19 +51,13 @@ def _worker(rank, world, port, ids, q):
         dist.destroy_process_group()
 
 
-def _free_port():
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        return s.getsockname()[1]
-
-
 @pytest.mark.parametrize("ids", [list(range(5)), [7, 3, 9, 1]])
-def test_allreduce_sums_every_shot_once(ids):
+def test_allreduce_sums_every_shot_once(ids, tmp_path):
     world = 2
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, ids, q)) for r in range(world)]
+    store = str(tmp_path / "rendezvous")
+    procs = [ctx.Process(target=_worker, args=(r, world, store, ids, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = [q.get(timeout=120) for _ in range(world)]
