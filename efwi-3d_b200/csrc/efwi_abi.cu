@@ -116,6 +116,9 @@ struct EfwiHandle {
   long long ck_forward_steps = 0;   // forward steps of the last exact gradient
   // optional outputs of the misfit: windowed synthetics / observed data
   float *scr_syn = nullptr, *scr_obs = nullptr, *scr_res = nullptr;
+  // optional output of exact gradients: dJ/dstf [n][nt] of the call's shots
+  float *gstf = nullptr;
+  DevBuf stf_w2;  // taper factor w^2 of the source-time functions [nt]
   DevBuf scr_tm;
   int ck_slots = 0;                 // slots it used
 
@@ -630,7 +633,7 @@ ExactArgs exact_args(EfwiHandle *h, const Fields &f, const Psi &ps, const Fields
 // is injected as it is, so the images are J^T applied to it.
 int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res_out,
                float *glam, float *gmu, float *gB, cudaStream_t st, bool adj_source = false,
-               long long scratch_off = 0) {
+               long long scratch_off = 0, float *gstf_row = nullptr) {
   const int nt = h->grid.nt;
   const int ntl = nt_eff(h);
   const long long N = h->N;
@@ -714,6 +717,13 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
               h->res_tm.as<float>(), res_out, nt, sh.nrec);
           h->launches[K_OTHER]++;
         }
+      }
+      if (k <= ntl - 2 && gstf_row) {
+        // the source of step k adds to the stresses after the stress stage
+        // of step k: its adjoint is read before that stage's transpose
+        k_stf_gradient<<<1, 32, 0, st>>>(a, b.src.cell, h->stf_w2.as<float>(), gstf_row, k,
+                                         2250000.0f * h->grid.dt);
+        h->launches[K_OTHER]++;
       }
       if (k <= ntl - 2) {
         Timer t(h, K_ADJ_STRESS, st, k);
@@ -915,6 +925,12 @@ int efwi_set_survey(EfwiHandle *h, int nshot, const EfwiShot *shots, const float
     }
     o.src_w = s.src_weight;
   }
+  {
+    std::vector<float> ones(g.nt, 1.0f), w2(g.nt);
+    taper_stf(ones.data(), g.nt, g.dt, w2.data());
+    CK_CUDA(h, h->stf_w2.ensure(sizeof(float) * g.nt));
+    CK_CUDA(h, cudaMemcpy(h->stf_w2.p, w2.data(), sizeof(float) * g.nt, cudaMemcpyHostToDevice));
+  }
   std::vector<float> tap((size_t)nshot * g.nt);
   for (int k = 0; k < nshot; ++k) taper_stf(stf + (size_t)k * g.nt, g.nt, g.dt, tap.data() + (size_t)k * g.nt);
   if (nshot > 0) {
@@ -989,8 +1005,10 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
   if (grad && mode == EFWI_MODE_EXACT) {
     for (int k = 0; k < n; ++k) {
       const ShotHost &sh = h->shots[ids[k]];
+      float *grow = h->gstf ? h->gstf + (size_t)k * nt : nullptr;
+      if (grow) CK_CUDA(h, cudaMemsetAsync(grow, 0, sizeof(float) * nt, st));
       int rc = exact_shot(h, ids[k], obs + obs_off, jdev + k, res_out ? res_out + obs_off : nullptr,
-                          glam, gmu, grho, st, adj_source, obs_off);
+                          glam, gmu, grho, st, adj_source, obs_off, grow);
       if (rc) return rc;
       obs_off += 3LL * sh.nrec * nt;
     }
@@ -1371,6 +1389,12 @@ int efwi_illumination(EfwiHandle *h, int n, const int *ids, float *h_lam, float 
   rc = check_launch(h, "illumination");
   if (rc) return rc;
   return status_check(h, st);
+}
+
+int efwi_set_stf_gradient(EfwiHandle *h, float *g_stf) {
+  if (!h) return EFWI_ERR_ARG;
+  h->gstf = g_stf;
+  return EFWI_OK;
 }
 
 int efwi_set_scratch(EfwiHandle *h, float *syn_w, float *obs_w, float *res) {

@@ -646,6 +646,18 @@ void launch_adj_velocity_exact(int bx, dim3 grid, cudaStream_t st, const ExactAr
     k_adj_velocity_exact<4><<<grid, dim3(32, 4), 0, st>>>(A, zchunk, nzc);
 }
 
+// dJ/dstf of step k: the source adds 1500^2 * dt * w^2(k) * stf(k) to szz,
+// sxx and syy at the source cell after the stress stage of step k
+// (utilities.cu:442-479, taper Src_Rec.cu:146), so its derivative is that
+// factor times the adjoint of the three stresses there at that point.
+__global__ void k_stf_gradient(Fields a, const long long *src_cell, const float *w2, float *out,
+                               int k, float scale) {
+  if (threadIdx.x != 0) return;
+  const long long i = src_cell[0];
+  if (i < 0) return;
+  out[k] = scale * w2[k] * (a.szz[i] + a.sxx[i] + a.syy[i]);
+}
+
 // rho image from the buoyancy image: B = 1/rho on [2, n-3]^3
 // (Model.cu:65-76), so dJ/drho = -dJ/dB * B^2 there and 0 elsewhere.
 __global__ void k_buoy_to_rho(const float *gB, const float *buoy, float *grho, int nz, int nx,

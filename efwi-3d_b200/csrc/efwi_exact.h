@@ -24,6 +24,8 @@ void launch_adj_velocity_exact(int bx, dim3 grid, cudaStream_t st, const ExactAr
 
 __global__ void k_buoy_to_rho(const float *gB, const float *buoy, float *grho, int nz, int nx,
                               int ny, int py);
+__global__ void k_stf_gradient(Fields a, const long long *src_cell, const float *w2, float *out,
+                               int k, float scale);
 __global__ void k_state_convert(Geo g, float *full, Fields f, Psi ps, int to_engine);
 __global__ void k_illumination(Geo g, Fields f, Psi ps, int S, const float *buoy, int do_stress,
                                float *hl, float *hm, float *hb);

@@ -85,6 +85,7 @@ _SIGS = {
                                C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_illumination": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p]),
+    "efwi_set_stf_gradient": (C.c_int, [C.c_void_p, C.c_void_p]),
     "efwi_set_scratch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_set_checkpoint_budget": (C.c_int, [C.c_void_p, C.c_longlong]),
     "efwi_state_bytes": (C.c_longlong, [C.c_void_p]),

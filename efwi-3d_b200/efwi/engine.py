@@ -232,6 +232,18 @@ class Propagator:
             return J.value, gl, gm, gr, res
         return J.value, gl, gm, gr
 
+    def stf_gradient(self, shot_ids, obs: torch.Tensor):
+        """Exact misfit gradient with respect to the (untapered) source-time
+        functions of the shots, [n, nt], besides J and the model images."""
+        ids = self._ids(shot_ids)
+        gs = torch.zeros(len(ids), self.grid.nt, device=self.device, dtype=torch.float32)
+        check(self._h, self._L.efwi_set_stf_gradient(self._h, C.c_void_p(gs.data_ptr())))
+        try:
+            out = self.gradient(shot_ids, obs, mode="exact")
+        finally:
+            check(self._h, self._L.efwi_set_stf_gradient(self._h, C.c_void_p(0)))
+        return out + (gs,)
+
     def set_scratch(self, syn_w=None, obs_w=None, res=None) -> None:
         """Device buffers (traces layout of the next calls' obs) that every
         misfit also fills with windowed synthetics, windowed observed data

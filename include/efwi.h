@@ -121,8 +121,8 @@ int efwi_gradient(EfwiHandle *h, int n, const int *shot_ids, const float *obs, i
                   double *misfit, float *g_lam, float *g_mu, float *g_rho, float *res,
                   void *stream);
 
-/* Shot windows (config 4 of the build's benchmarks; no reference
- * counterpart): shot k runs on its own aperture window of the padded grid,
+/* Shot windows (no reference counterpart): shot k runs on its own aperture
+ * window of the padded grid,
  * x in [x0, x0 + nx), y in [y0, y0 + ny), all z, with its own C-PML of npml
  * cells inside the window edges; receivers outside the window record
  * zeros.  All windows of a call advance together in one persistent launch
@@ -178,6 +178,13 @@ int efwi_checkpoint_plan(int nt, int slots, long long *forward_steps, int *slots
  * (full grids; only their C-PML slabs are read and written).  No reference
  * counterpart; it serves dot-product tests of the adjoint. */
 int efwi_step(EfwiHandle *h, float *state, int transpose, void *stream);
+
+/* Source-time-function gradient (the reference returns zeros,
+ * Torch_Fwi.cpp:73,96): while g_stf (device [n][nt]) is set, every
+ * EFWI_MODE_EXACT gradient also writes dJ/dstf of its n shots, row k for
+ * shot_ids[k], with respect to the untapered stf rows given to
+ * efwi_set_survey.  NULL disables. */
+int efwi_set_stf_gradient(EfwiHandle *h, float *g_stf);
 
 /* Scratch outputs (the reference's scratch_dir_name dumps,
  * libCUFD.cu:660-700): while set, every misfit of efwi_misfit /
