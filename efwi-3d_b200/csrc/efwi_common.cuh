@@ -77,14 +77,16 @@ __device__ __forceinline__ bool slab_v(int i, int n, int np) { return i < np || 
 
 __device__ __forceinline__ int slab_c(int i, int n, int np) { return i < np ? i : i - (n - 2 * np); }
 
-__device__ __forceinline__ long long psi_z_idx(const Geo &g, int z, int x, int y) {
-  return ((long long)slab_c(z, g.nz, g.np) * g.nx + x) * g.ny + y;
+// Offsets within one slab variable; 32-bit, as a slab holds fewer cells
+// than a volume (fewer than 2^31, checked by efwi_create).
+__device__ __forceinline__ int psi_z_idx(const Geo &g, int z, int x, int y) {
+  return (slab_c(z, g.nz, g.np) * g.nx + x) * g.ny + y;
 }
-__device__ __forceinline__ long long psi_x_idx(const Geo &g, int z, int x, int y) {
-  return ((long long)z * (2 * g.np) + slab_c(x, g.nx, g.np)) * g.ny + y;
+__device__ __forceinline__ int psi_x_idx(const Geo &g, int z, int x, int y) {
+  return (z * (2 * g.np) + slab_c(x, g.nx, g.np)) * g.ny + y;
 }
-__device__ __forceinline__ long long psi_y_idx(const Geo &g, int z, int x, int y) {
-  return ((long long)z * g.nx + x) * (2 * g.np) + slab_c(y, g.ny, g.np);
+__device__ __forceinline__ int psi_y_idx(const Geo &g, int z, int x, int y) {
+  return (z * g.nx + x) * (2 * g.np) + slab_c(y, g.ny, g.np);
 }
 
 // Reads of adjoint memory variables at neighbours: zero outside the slab
