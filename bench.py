@@ -45,7 +45,10 @@ def parse():
     ap.add_argument("--profile-sample", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-nt", type=int, default=24, help="time steps of the CPU samples")
+    ap.add_argument("--cpu-nt", type=int, default=160,
+                    help="time steps of the cpu_baseline sample (about 10-30 s of host work)")
+    ap.add_argument("--ref-nt", type=int, default=24,
+                    help="time steps of each sample of --impl reference (one per step)")
     ap.add_argument("--tile-bx", type=int, default=4)
     ap.add_argument("--zchunk", type=int, default=8)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
@@ -216,7 +219,7 @@ def run_reference(a):
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref (reference kernels built for the host) is missing"}))
         return
-    cs = CpuSample("ref", a.n, a.cpu_nt)
+    cs = CpuSample("ref", a.n, a.ref_nt)
     for _ in range(a.warmup):
         cs.run()
     rates, els = [], []
@@ -226,11 +229,11 @@ def run_reference(a):
         els.append(el)
     v = sum(rates) / len(rates)
     p, cores = cs.p, cs.cores
-    sample = f"1 shot of the {p.grid.nz}^3 padded grid, nt={a.cpu_nt}, reference gradient (calc_id 1)"
+    sample = f"1 shot of the {p.grid.nz}^3 padded grid, nt={a.ref_nt}, reference gradient (calc_id 1)"
     line = dict(base)
     line.update({"value": v, "ms_per_step": 1e3 * sum(els) / len(els),
                  "config": {"workload": "config2 sample: " + sample, "model_cells": a.n,
-                            "padded": p.grid.nz, "shots_per_step": 1, "nt": a.cpu_nt},
+                            "padded": p.grid.nz, "shots_per_step": 1, "nt": a.ref_nt},
                  "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                                   "sample": sample},
                  "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
