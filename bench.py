@@ -167,6 +167,14 @@ def kernel_bytes(grid, nshot_launch=1):
     return {k: v * nshot_launch for k, v in per.items()}
 
 
+# DRAM bytes (read + write) per launch of the stencil kernels on the 152^3
+# padded grid (128^3 model, C-PML 12), one shot per launch, from one ncu
+# capture each (profiles/stencil_rev_tma_config2.md,
+# profiles/stencil_fwd_tma_config2.md); other grids report no traffic.
+TRAFFIC_152 = {"rev_velocity": 415.4e6, "rev_stress": 501.3e6,
+               "stress_fwd": 221.6e6, "velocity_fwd": 184.4e6}
+
+
 def algorithmic_step_bytes(grid, nmodel):
     """B_g = 3 B_f + 24 N_int per time step, B_f = 120 N + 48 S."""
     n = grid.ncell
@@ -555,8 +563,11 @@ def main():
     if dom:
         avg_s = prof[dom]["ms"] / prof[dom]["timed"] * 1e-3
         ach = kb[dom] / avg_s / 1e9
+        tr = TRAFFIC_152.get(dom) if (g.nz, g.nx, g.ny, g.npml) == (152, 152, 152, 12) else None
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": tr,
+                "traffic_source": "ncu capture, one launch (profiles/)" if tr else None,
+                "algorithmic_bytes": kb[dom],
                 "peak_kind": peak_kind, "avg_launch_ms": round(avg_s * 1e3, 4),
                 "shares": {k: round(v / sum(tot_ms.values()), 4) for k, v in tot_ms.items()}}
     nmodel = (g.nz - 2 * g.npml) * (g.nx - 2 * g.npml) * (g.ny - 2 * g.npml)
