@@ -83,6 +83,9 @@ k_stress_fwd_tma(const __grid_constant__ Maps<11> maps, Geo g, Fields f, Psi ps,
     float hz = 0.f, hx = 0.f, hy = 0.f;
     if (act && q + 1 < nq) {
       hz = vz[i + 2 * sz]; hx = vx[i + 3 * sz]; hy = vy[i + 3 * sz];
+      if (q + 2 < nq) {  // heads of the plane after next (z + 4 <= nz - 1)
+        prefetch_l2(vz + i + 3 * sz); prefetch_l2(vx + i + 4 * sz); prefetch_l2(vy + i + 4 * sz);
+      }
     }
     const bool got = ring.wait(q);
     if (act && got) {
@@ -225,6 +228,9 @@ k_velocity_fwd_tma(const __grid_constant__ Maps<9> maps, Geo g, Fields f, Psi ps
     float ha = 0.f, hb = 0.f, hc = 0.f;
     if (act && q + 1 < nq) {
       ha = szz[i + 3 * sz]; hb = sxz[i + 2 * sz]; hc = syz[i + 2 * sz];
+      if (q + 2 < nq) {
+        prefetch_l2(szz + i + 4 * sz); prefetch_l2(sxz + i + 3 * sz); prefetch_l2(syz + i + 3 * sz);
+      }
     }
     const bool got = ring.wait(q);
     if (act && got) {

@@ -139,6 +139,15 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
         h3 = a.szz[i + 3 * sz]; h4 = a.sxx[i + 3 * sz]; h5 = a.syy[i + 3 * sz];
         h6 = a.sxz[i + 2 * sz]; h7 = a.syz[i + 2 * sz];
       }
+      if (q + 2 < nq) {  // heads of the plane after next (z + 4 <= nz - 1)
+        if (L::REV) {
+          prefetch_l2(f.szz + i + 4 * sz); prefetch_l2(f.sxz + i + 3 * sz); prefetch_l2(f.syz + i + 3 * sz);
+        }
+        if (L::ADJ) {
+          prefetch_l2(a.szz + i + 4 * sz); prefetch_l2(a.sxx + i + 4 * sz); prefetch_l2(a.syy + i + 4 * sz);
+          prefetch_l2(a.sxz + i + 3 * sz); prefetch_l2(a.syz + i + 3 * sz);
+        }
+      }
     }
     const bool got = ring.wait(q);
     if (act && got) {
@@ -296,6 +305,10 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
     if (act && q + 1 < nq) {
       h0 = f.vz[i + 2 * sz]; h1 = f.vx[i + 3 * sz]; h2 = f.vy[i + 3 * sz];
       h3 = a.vz[i + 2 * sz]; h4 = a.vx[i + 3 * sz]; h5 = a.vy[i + 3 * sz];
+      if (q + 2 < nq) {
+        prefetch_l2(f.vz + i + 3 * sz); prefetch_l2(f.vx + i + 4 * sz); prefetch_l2(f.vy + i + 4 * sz);
+        prefetch_l2(a.vz + i + 3 * sz); prefetch_l2(a.vx + i + 4 * sz); prefetch_l2(a.vy + i + 4 * sz);
+      }
     }
     const bool got = ring.wait(q);
     if (act && got) {

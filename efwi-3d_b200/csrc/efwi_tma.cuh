@@ -58,6 +58,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
 // One try: the thread may be suspended up to TMA_SUSPEND_NS while the
 // phase is incomplete, instead of spinning and taking issue slots.
 constexpr uint32_t TMA_SUSPEND_NS = 2000;
+// Hint that the line holding *p will be read soon: bring it into L2 (no
+// register is written; the z-queue heads of the next plane use it).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
