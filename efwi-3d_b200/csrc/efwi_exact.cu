@@ -56,11 +56,6 @@ __device__ __forceinline__ int psi32_y(const Geo &g, int z, int x, int y) {
   return (z * g.nx + x) * (2 * g.np) + slab_c(y, g.ny, g.np);
 }
 
-// Brings the line of *p into L2 ahead of its load (no register written).
-__device__ __forceinline__ void pf_l2(const float *p) {
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
 __device__ __forceinline__ float qpml(float G, bool slab, float L, float kinv, float a) {
   return slab ? G * kinv + a * (L + G) : G;
 }
@@ -235,13 +230,6 @@ __global__ void __launch_bounds__(32 * BX) k_adj_stress_exact(ExactArgs A, int z
   for (int z = z0; z < z1; ++z, buf ^= 1) {
     qez[4] = qvx[4] = qvy[4] = 0.f;
     if (act) qs_z(A, z + 2, x, y, qez[4], qvx[4], qvy[4]);
-    if (act && z + 4 < nz) {  // next plane's z-queue inputs
-      const int j = cell32(g, z + 3, x, y);
-      pf_l2(A.a.szz + j); pf_l2(A.a.sxx + j); pf_l2(A.a.syy + j);
-      pf_l2(A.a.sxz + j); pf_l2(A.a.sxy + j); pf_l2(A.a.syz + j);
-      pf_l2(A.lam + j); pf_l2(A.mu + j);
-      pf_l2(A.f.vz + j); pf_l2(A.f.vx + j + sz); pf_l2(A.f.vy + j + sz);
-    }
     float ox[3] = {0.f, 0.f, 0.f}, oy[3] = {0.f, 0.f, 0.f};
     GS G{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (act) G = qs_own(A, z, x, y, ox, oy);
@@ -517,11 +505,6 @@ __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int
   for (int z = z0; z < z1; ++z, buf ^= 1) {
     qzz[4] = qxz[4] = qyz[4] = 0.f;
     if (act) qv_z(A, z + 2, x, y, qzz[4], qxz[4], qyz[4]);
-    if (act && z + 4 < nz) {  // next plane's z-queue inputs
-      const int j = cell32(g, z + 3, x, y);
-      pf_l2(A.a.vz + j); pf_l2(A.a.vx + j); pf_l2(A.a.vy + j); pf_l2(A.buoy + j);
-      pf_l2(A.f.szz + j + sz); pf_l2(A.f.sxz + j); pf_l2(A.f.syz + j);
-    }
     float ox[3] = {0.f, 0.f, 0.f}, oy[3] = {0.f, 0.f, 0.f};
     float gz = 0.f, gx = 0.f, gy = 0.f;
     if (act) qv_own(A, z, x, y, gz, gx, gy, ox, oy);
