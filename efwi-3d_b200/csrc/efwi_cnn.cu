@@ -10,10 +10,9 @@
 // The convolution is an implicit GEMM: per output voxel row of 16
 // consecutive x, one warp accumulates sum over taps t and input channels of
 // X[v + off_t][ci] W[t][co][ci] with mma.m16n8k16 (bf16 in, f32 accumulate):
-// A = 16 voxels x 16 input channels of one tap (one 32-bit load per
-// register: the two channels of a register are adjacent), B = 16 input
-// channels x 8 output channels, two n-tiles.  Voxels outside the volume
-// read as zero.
+// A = 16 voxels x 16 input channels of one tap (ldmatrix from the CTA's
+// staged input tile), B = 16 input channels x 8 output channels, two
+// n-tiles.  Voxels outside the volume read as zero.
 //
 //   k_conv3d_fwd     y = act(conv(x, W) + b), stored as bf16 and/or f32.
 //                    With W'[t][a][b] = W[26-t][b][a] it also computes the
@@ -45,43 +44,62 @@ __device__ __forceinline__ uint32_t ld16(const __nv_bfloat16 *p) {
 }
 
 constexpr int kC = 16;              // channels
-constexpr int kWarpsFwd = 4;        // warps per CTA of k_conv3d_fwd
+constexpr int kRowsFwd = 8;   // warps per CTA of k_conv3d_fwd: one y row each
+constexpr int kTileX = 16;    // voxels per warp row
+constexpr int kVoxPitch = 48; // bytes per staged voxel (32 of data): ldmatrix rows hit
+                              // distinct banks
+constexpr int kTileVox = 3 * (kRowsFwd + 2) * (kTileX + 2);
 
-__global__ void __launch_bounds__(32 * kWarpsFwd)
+__device__ __forceinline__ void ldmatrix_x4(uint32_t a[4], uint32_t addr) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+               : "r"(addr));
+}
+
+// A CTA computes the voxels (z, y0 .. y0+7, x0 .. x0+15).  Its input with a
+// 1-voxel halo (3 x 10 x 18 voxels) is staged in shared memory once; each
+// warp then takes, per tap, the 16 x 16 A fragment of its row with one
+// ldmatrix.x4 (matrices: voxels 0-7 / 8-15 x channels 0-7 / 8-15, which is
+// the register order of the mma A operand).
+__global__ void __launch_bounds__(32 * kRowsFwd)
 k_conv3d_fwd(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
              const float *__restrict__ bias, int D, int H, int W, int relu,
              __nv_bfloat16 *__restrict__ yb, float *__restrict__ yf) {
-  __shared__ uint32_t sw[27 * kC * kC / 2];  // [t][co][ci pair]
-  for (int k = threadIdx.x; k < 27 * kC * kC / 2; k += blockDim.x) sw[k] = ld32(w + 2 * k);
+  __shared__ __align__(16) uint32_t sw[27 * kC * kC / 2];  // [t][co][ci pair]
+  __shared__ __align__(16) unsigned char sx[kTileVox * kVoxPitch];
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kRowsFwd, z = blockIdx.z;
+  for (int k = tid; k < 27 * kC * kC / 2; k += blockDim.x) sw[k] = ld32(w + 2 * k);
+  for (int c = tid; c < 2 * kTileVox; c += blockDim.x) {
+    const int v = c >> 1, h = c & 1;
+    const int xx = v % (kTileX + 2), t = v / (kTileX + 2);
+    const int yy = t % (kRowsFwd + 2), zz = t / (kRowsFwd + 2);
+    const int gz = z - 1 + zz, gy = y0 - 1 + yy, gx = x0 - 1 + xx;
+    uint4 val = make_uint4(0u, 0u, 0u, 0u);
+    if (gz >= 0 && gz < D && gy >= 0 && gy < H && gx >= 0 && gx < W)
+      val = *reinterpret_cast<const uint4 *>(x + (((long long)gz * H + gy) * W + gx) * kC + h * 8);
+    *reinterpret_cast<uint4 *>(sx + v * kVoxPitch + h * 16) = val;
+  }
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int y = y0 + warp;
+  if (y >= H) return;  // no barrier follows
   const int g = lane >> 2, q = lane & 3;
-  const int nxc = (W + 15) >> 4;
-  const long long unit = (long long)blockIdx.x * kWarpsFwd + warp;
-  if (unit >= (long long)D * H * nxc) return;
-  const int xc = (int)(unit % nxc);
-  const long long zy = unit / nxc;
-  const int y = (int)(zy % H), z = (int)(zy / H);
-  const int x0 = xc * 16;
+  const uint32_t sxa = (uint32_t)__cvta_generic_to_shared(sx);
+  const int lrow = ((lane >> 3) & 1) * 8 + (lane & 7);  // voxel of this lane's ldmatrix row
+  const int lcol = (lane >> 4) * 16;                      // channel half (bytes)
 
   float c[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-  for (int dz = -1; dz <= 1; ++dz) {
-    const int zz = z + dz;
-    if (zz < 0 || zz >= D) continue;
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int yy = y + dy;
-      if (yy < 0 || yy >= H) continue;
-      const __nv_bfloat16 *row = x + ((long long)zz * H + yy) * W * kC;
 #pragma unroll
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int t = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-        const int r0 = x0 + g + dx, r1 = r0 + 8;
-        const bool v0 = r0 >= 0 && r0 < W, v1 = r1 >= 0 && r1 < W;
+  for (int dz = 0; dz < 3; ++dz) {
+#pragma unroll
+    for (int dy = 0; dy < 3; ++dy) {
+#pragma unroll
+      for (int dx = 0; dx < 3; ++dx) {
+        const int t = dz * 9 + dy * 3 + dx;
+        const int v0 = (dz * (kRowsFwd + 2) + warp + dy) * (kTileX + 2) + dx;
         uint32_t a[4];
-        a[0] = v0 ? ld32(row + r0 * kC + 2 * q) : 0u;
-        a[1] = v1 ? ld32(row + r1 * kC + 2 * q) : 0u;
-        a[2] = v0 ? ld32(row + r0 * kC + 2 * q + 8) : 0u;
-        a[3] = v1 ? ld32(row + r1 * kC + 2 * q + 8) : 0u;
+        ldmatrix_x4(a, sxa + (uint32_t)((v0 + lrow) * kVoxPitch + lcol));
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt) {
           const uint32_t *wb = sw + (t * kC + nt * 8 + g) * (kC / 2);
@@ -96,10 +114,10 @@ k_conv3d_fwd(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restric
     const int co = nt * 8 + 2 * q;
     const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int xv = x0 + g + 8 * h;
+    for (int hh = 0; hh < 2; ++hh) {
+      const int xv = x0 + g + 8 * hh;
       if (xv >= W) continue;
-      float o0 = c[nt][2 * h] + b0, o1 = c[nt][2 * h + 1] + b1;
+      float o0 = c[nt][2 * hh] + b0, o1 = c[nt][2 * hh + 1] + b1;
       if (relu) { o0 = fmaxf(o0, 0.f); o1 = fmaxf(o1, 0.f); }
       const long long off = (((long long)z * H + y) * W + xv) * kC + co;
       if (yb) *reinterpret_cast<__nv_bfloat162 *>(yb + off) = __floats2bfloat162_rn(o0, o1);
@@ -184,11 +202,10 @@ using namespace efwi;
 
 extern "C" int efwi_conv3d_forward(const void *x, const void *w, const float *bias, int D, int H,
                                    int W, int relu, void *y_bf16, float *y_f32, void *stream) {
-  if (!x || !w || D < 1 || H < 1 || W < 1 || (!y_bf16 && !y_f32)) return 1;
-  const long long units = (long long)D * H * ((W + 15) / 16);
-  const long long blocks = (units + kWarpsFwd - 1) / kWarpsFwd;
-  if (blocks > 0x7fffffffLL) return 1;
-  k_conv3d_fwd<<<(unsigned)blocks, 32 * kWarpsFwd, 0, (cudaStream_t)stream>>>(
+  if (!x || !w || D < 1 || H < 1 || W < 1 || D > 65535 || (!y_bf16 && !y_f32)) return 1;
+  if (((uintptr_t)x & 15) != 0) return 1;  // staged with 16-byte loads
+  const dim3 grid((W + kTileX - 1) / kTileX, (H + kRowsFwd - 1) / kRowsFwd, D);
+  k_conv3d_fwd<<<grid, 32 * kRowsFwd, 0, (cudaStream_t)stream>>>(
       (const __nv_bfloat16 *)x, (const __nv_bfloat16 *)w, bias, D, H, W, relu,
       (__nv_bfloat16 *)y_bf16, y_f32);
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
