@@ -112,6 +112,9 @@ struct EfwiHandle {
   // shot windows: per-domain volumes and tables; stream for graph capture
   DevBuf wvol, wtab;
   cudaStream_t cap_stream = nullptr;
+  // shot windows on the TMA kernels: window groups run on their own streams
+  cudaStream_t wst[8] = {};
+  cudaEvent_t wev[9] = {};
   long long ck_budget = 4LL << 30;  // bytes of checkpoint slots
   long long ck_forward_steps = 0;   // forward steps of the last exact gradient
   // optional outputs of the misfit: windowed synthetics / observed data
@@ -285,13 +288,15 @@ int get_encoder(EfwiHandle *h) {
 
 // Tensor map of S stacked pitched volumes [S*nz][nx][py]; halo boxes of
 // 40 (y) x (bx + 4) (x) x 1 plane, or point boxes of 32 x bx x 1.
-int make_map(EfwiHandle *h, CUtensorMap *m, const float *base, int S, bool halo, int bx) {
+// Tensor map of one field over volumes of pitch py, nx rows and nzs planes.
+int make_map_dims(EfwiHandle *h, CUtensorMap *m, const float *base, int py, int nx, long long nzs,
+                  bool halo, int bx) {
   int rc = get_encoder(h);
   if (rc) return rc;
-  if (((uintptr_t)base & 15) != 0 || (h->py & 3) != 0)
+  if (((uintptr_t)base & 15) != 0 || (py & 3) != 0)
     return fail(h, EFWI_ERR_ARG, "tensor map base or pitch not 16-byte aligned");
-  cuuint64_t dims[3] = {(cuuint64_t)h->py, (cuuint64_t)h->grid.nx, (cuuint64_t)h->grid.nz * S};
-  cuuint64_t strides[2] = {(cuuint64_t)h->py * 4, (cuuint64_t)h->grid.nx * h->py * 4};
+  cuuint64_t dims[3] = {(cuuint64_t)py, (cuuint64_t)nx, (cuuint64_t)nzs};
+  cuuint64_t strides[2] = {(cuuint64_t)py * 4, (cuuint64_t)nx * py * 4};
   cuuint32_t box[3] = {halo ? (cuuint32_t)TMA_BOXY : 32u,
                        (cuuint32_t)(halo ? bx + 2 * TMA_HX : bx), 1};
   cuuint32_t es[3] = {1, 1, 1};
@@ -300,6 +305,10 @@ int make_map(EfwiHandle *h, CUtensorMap *m, const float *base, int S, bool halo,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(h, EFWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return EFWI_OK;
+}
+
+int make_map(EfwiHandle *h, CUtensorMap *m, const float *base, int S, bool halo, int bx) {
+  return make_map_dims(h, m, base, h->py, h->grid.nx, (long long)h->grid.nz * S, halo, bx);
 }
 
 // Resets the status word at the start of a call.
@@ -745,6 +754,129 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
   return check_launch(h, "exact gradient");
 }
 
+// Traces of the windows (time-major, per window at trace_off) into the
+// caller's [3][nrec][nt] layout per shot; synchronises the stream.
+int window_traces(EfwiHandle *h, const std::vector<Domain> &dom, float *traces, cudaStream_t st) {
+  const int nt = h->grid.nt;
+  const float *ttm = h->traces_tm.as<float>();
+  long long off = 0;
+  for (const Domain &d : dom) {
+    if (d.nrec > 0) {
+      k_traces_to_cr_t<<<dim3((nt + 31) / 32, (d.nrec + 31) / 32, 3), dim3(32, 8), 0, st>>>(
+          ttm + d.trace_off, traces + off, nt, d.nrec);
+      h->launches[K_OTHER]++;
+    }
+    off += 3LL * d.nrec * nt;
+  }
+  int rc = check_launch(h, "window forward");
+  if (rc) return rc;
+  CK_CUDA(h, cudaStreamSynchronize(st));
+  return EFWI_OK;
+}
+
+// Tensor maps of the forward TMA kernels over one window's state and
+// sliced model.
+int make_window_maps(EfwiHandle *h, const Domain &d, int bxf, FwdMaps *maps) {
+  const Fields &f = d.f;
+  const float *sm[11] = {f.vz, f.vx, f.vy, f.szz, f.sxx, f.syy, f.sxz, f.sxy, f.syz, d.lam, d.mu};
+  const float *vm[9] = {f.sxz, f.syz, f.sxx, f.sxy, f.syy, f.vz, f.vx, f.vy, d.buoy};
+  for (int k = 0; k < 11; ++k) {
+    int rc = make_map_dims(h, &maps->s.m[k], sm[k], d.g.sx, d.g.nx, d.g.nz, k < 3, bxf);
+    if (rc) return rc;
+  }
+  for (int k = 0; k < 9; ++k) {
+    int rc = make_map_dims(h, &maps->v.m[k], vm[k], d.g.sx, d.g.nx, d.g.nz, k < 5, bxf);
+    if (rc) return rc;
+  }
+  return EFWI_OK;
+}
+
+// Time loop of the windows on the TMA kernels.  Each window is its own
+// single-domain grid with its own tensor maps (kernel parameters, which a
+// table of many domains in one launch cannot carry).  Contiguous groups of
+// windows, balanced by cells, advance on up to 8 streams (the default
+// number of hardware queues); every group records its own receivers after
+// its velocity updates, so the groups never wait on one another inside the
+// loop.  Each launch covers a whole window, so one stream already fills the
+// GPU; the other streams fill the tails between launches.
+int window_loop_tma(EfwiHandle *h, const std::vector<Domain> &dom, const std::vector<int> &rec_dom,
+                    const Domain *ddom, const int *drd, const int *drc, const int *drr,
+                    long long *dsrc, float *ttm, int ntl, cudaStream_t st) {
+  const int n = (int)dom.size();
+  int rc = status_reset(h, st);
+  if (rc) return rc;
+  std::vector<long long> srcs(n);
+  for (int k = 0; k < n; ++k) srcs[k] = dom[k].src_cell;
+  CK_CUDA(h, cudaMemcpyAsync(dsrc, srcs.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, st));
+  const int bxf = fwd_tma_tile(h->fcfg);
+  std::vector<FwdMaps> maps(n);
+  for (int k = 0; k < n; ++k) {
+    rc = make_window_maps(h, dom[k], bxf, &maps[k]);
+    if (rc) return rc;
+  }
+  // groups [gbeg[g], gbeg[g+1]) of at least one window each
+  const int G = std::min(n, 8);
+  std::vector<long long> cum(n + 1, 0);
+  for (int k = 0; k < n; ++k) cum[k + 1] = cum[k] + dom[k].g.N;
+  std::vector<int> gbeg(G + 1, n);
+  gbeg[0] = 0;
+  for (int g = 1; g < G; ++g) {
+    int k = gbeg[g - 1] + 1;
+    while (k < n - (G - g) && cum[k] * G < cum[n] * g) ++k;
+    gbeg[g] = k;
+  }
+  // receivers are listed window by window: rstart[k] is window k's first
+  std::vector<int> rstart(n + 1, 0);
+  for (int d : rec_dom) rstart[d + 1]++;
+  for (int k = 0; k < n; ++k) rstart[k + 1] += rstart[k];
+  for (int g = 0; g < G; ++g)
+    if (!h->wst[g]) CK_CUDA(h, cudaStreamCreateWithFlags(&h->wst[g], cudaStreamNonBlocking));
+  for (int e = 0; e < 9; ++e)
+    if (!h->wev[e]) CK_CUDA(h, cudaEventCreateWithFlags(&h->wev[e], cudaEventDisableTiming));
+  CK_CUDA(h, cudaEventRecord(h->wev[8], st));
+  for (int g = 0; g < G; ++g) CK_CUDA(h, cudaStreamWaitEvent(h->wst[g], h->wev[8], 0));
+  int *status = h->status.as<int>();
+  const int nt = h->grid.nt;
+  std::vector<dim3> grids(n);
+  std::vector<int> nzcs(n);
+  for (int k = 0; k < n; ++k) {
+    const Geo &g = dom[k].g;
+    nzcs[k] = (g.nz + h->zchunk - 1) / h->zchunk;
+    grids[k] = dim3((g.ny + 31) / 32, (g.nx + bxf - 1) / bxf, nzcs[k]);
+  }
+  long long nrec_launch = 0;
+  for (int it = 0; it <= ntl - 2; ++it) {
+    for (int g = 0; g < G; ++g) {
+      cudaStream_t s = h->wst[g];
+      for (int k = gbeg[g]; k < gbeg[g + 1]; ++k) {
+        const Domain &d = dom[k];
+        const SrcArgs src{dsrc + k, d.stf, nt, it};
+        launch_stress_fwd_tma(h->fcfg, grids[k], s, maps[k].s, d.g, d.f, d.ps, h->zchunk, nzcs[k],
+                              src, status);
+        launch_velocity_fwd_tma(h->fcfg, grids[k], s, maps[k].v, d.g, d.f, d.ps, h->zchunk,
+                                nzcs[k], status);
+      }
+      const int r0 = rstart[gbeg[g]], r1 = rstart[gbeg[g + 1]];
+      if (r1 > r0) {
+        k_record_multi<<<(r1 - r0 + 127) / 128, 128, 0, s>>>(ddom, drd + r0, drc + r0, drr + r0,
+                                                               r1 - r0, ttm, it + 1);
+        ++nrec_launch;
+      }
+    }
+  }
+  for (int g = 0; g < G; ++g) {
+    CK_CUDA(h, cudaEventRecord(h->wev[g], h->wst[g]));
+    CK_CUDA(h, cudaStreamWaitEvent(st, h->wev[g], 0));
+  }
+  const long long steps = std::max(ntl - 1, 0);
+  h->launches[K_STRESS_FWD] += steps * n;
+  h->launches[K_VELOCITY_FWD] += steps * n;
+  h->launches[K_RECORD] += nrec_launch;
+  rc = check_launch(h, "window forward (TMA)");
+  if (rc) return rc;
+  return status_check(h, st);
+}
+
 }  // namespace
 
 extern "C" {
@@ -819,6 +951,10 @@ void efwi_destroy(EfwiHandle *h) {
   if (!h) return;
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+  for (cudaStream_t s : h->wst)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : h->wev)
+    if (e) cudaEventDestroy(e);
   delete h;
 }
 
@@ -1249,7 +1385,7 @@ int efwi_forward_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow 
   const long long nr = (long long)rec_dom.size();
   const size_t b_dom = ((sizeof(Domain) * n + 255) / 256) * 256, b_coef = sizeof(float) * coefs.size();
   const size_t b_rec = ((sizeof(int) * nr + 255) / 256) * 256;
-  CK_CUDA(h, h->wtab.ensure(b_dom + b_coef + 3 * b_rec + 256));
+  CK_CUDA(h, h->wtab.ensure(b_dom + b_coef + 3 * b_rec + sizeof(long long) * n + 256));
   char *tab = h->wtab.as<char>();
   float *dcoef = (float *)(tab + b_dom);
   int *drd = (int *)(tab + b_dom + b_coef), *drc = (int *)((char *)drd + b_rec),
@@ -1283,9 +1419,15 @@ int efwi_forward_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow 
   rc = check_launch(h, "window set-up");
   if (rc) return rc;
   const Domain *ddom = (const Domain *)tab;
-  const int blocks = multi_blocks(bx);
   const int ntl = nt_eff(h);
   float *ttm = h->traces_tm.as<float>();
+  if (h->variant == 1) {
+    long long *dsrc = (long long *)((char *)drr + b_rec);
+    rc = window_loop_tma(h, dom, rec_dom, ddom, drd, drc, drr, dsrc, ttm, ntl, st);
+    if (rc) return rc;
+    return window_traces(h, dom, traces, st);
+  }
+  const int blocks = multi_blocks(bx);
   auto loop = [&](cudaStream_t s) {
     for (int it = 0; it <= ntl - 2; ++it) {
       launch_fwd_multi(bx, blocks, s, ddom, n, tiles, zchunk, it);
@@ -1320,20 +1462,7 @@ int efwi_forward_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow 
   h->launches[K_STRESS_FWD] += ntl - 1;
   h->launches[K_VELOCITY_FWD] += ntl - 1;
   if (nr > 0) h->launches[K_RECORD] += ntl - 1;
-  long long off = 0;
-  for (int k = 0; k < n; ++k) {
-    const int nrs = dom[k].nrec;
-    if (nrs > 0) {
-      k_traces_to_cr_t<<<dim3((nt + 31) / 32, (nrs + 31) / 32, 3), dim3(32, 8), 0, st>>>(
-          ttm + dom[k].trace_off, traces + off, nt, nrs);
-      h->launches[K_OTHER]++;
-    }
-    off += 3LL * nrs * nt;
-  }
-  rc = check_launch(h, "window forward");
-  if (rc) return rc;
-  CK_CUDA(h, cudaStreamSynchronize(st));
-  return EFWI_OK;
+  return window_traces(h, dom, traces, st);
 }
 
 int efwi_adjoint(EfwiHandle *h, int n, const int *ids, const float *adj_src, float *g_lam,

@@ -65,25 +65,48 @@ def autotune(P, shot_id: int, obs_shot: torch.Tensor, nt_probe: int = 16,
             "rev_default_ms": round(rev.get((0, 8), float("nan")), 4), "probes": len(fwd) + len(rev)}
 
 
-def autotune_windows(P, shot_ids, windows, nt_probe: int = 16, bxs=(4, 8), zchunks=(4, 8, 16)):
-    """Launch shape (tile_bx, zchunk) of the multi-domain window launch: the
-    fastest over short probes (time loop stopped after `nt_probe` steps),
-    timed with CUDA events on the current stream; sets it on P."""
+def autotune_windows(P, shot_ids, windows, nt_probe: int = 16, bxs=(4, 8), zchunks=(4, 8, 16),
+                     fwd_cfgs: Sequence[int] = FWD_CFGS, tma_zchunks=(2, 4, 8)):
+    """Stencil variant and launch shape of the window forward, the fastest
+    over short probes (time loop stopped after `nt_probe` steps, CUDA events
+    on the current stream): the L1-served multi-domain launch over
+    (tile_bx, zchunk) and the per-window TMA kernels over (fwd_cfg, zchunk).
+    Sets the choice on P (its variant included: the windows' results do not
+    depend on it)."""
+    def probe():
+        P.forward_windows(shot_ids, windows, use_graph=True)  # warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P.forward_windows(shot_ids, windows, use_graph=True)
+        e1.record()
+        torch.cuda.synchronize(P.device)
+        return e0.elapsed_time(e1)
+
+    cur = getattr(P, "tuning", (0, 8, 0, 8))
     P.set_nt_limit(nt_probe)
     times = {}
     try:
+        P.set_variant(0)
         for bx, zc in itertools.product(bxs, zchunks):
             P.set_options(if_win=P.if_win, tile_bx=bx, zchunk=zc)
-            P.forward_windows(shot_ids, windows, use_graph=True)  # warm
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            P.forward_windows(shot_ids, windows, use_graph=True)
-            e1.record()
-            torch.cuda.synchronize(P.device)
-            times[(bx, zc)] = e0.elapsed_time(e1)
+            times[("l1", bx, zc)] = probe()
+        P.set_variant(1)
+        for cfg, zc in itertools.product(fwd_cfgs, tma_zchunks):
+            P.set_tuning(cfg, zc, cur[2], cur[3])
+            times[("tma", cfg, zc)] = probe()
     finally:
         P.set_nt_limit(0)
     best = min(times, key=times.get)
-    P.set_options(if_win=P.if_win, tile_bx=best[0], zchunk=best[1])
-    return {"tile_bx": best[0], "zchunk": best[1], "probe_ms": round(times[best], 3),
-            "probes": len(times)}
+    if best[0] == "l1":
+        P.set_variant(0)
+        P.set_options(if_win=P.if_win, tile_bx=best[1], zchunk=best[2])
+        out = {"variant": "l1", "tile_bx": best[1], "zchunk": best[2]}
+    else:
+        P.set_variant(1)
+        P.set_tuning(best[1], best[2], cur[2], cur[3])
+        out = {"variant": "tma", "fwd_cfg": best[1], "zchunk": best[2]}
+    best_l1 = min(v for k, v in times.items() if k[0] == "l1")
+    best_tma = min(v for k, v in times.items() if k[0] == "tma")
+    out.update({"probe_ms": round(times[best], 3), "best_l1_ms": round(best_l1, 3),
+                "best_tma_ms": round(best_tma, 3), "probes": len(times)})
+    return out

@@ -1,7 +1,8 @@
-"""Shot windows in one persistent multi-domain launch (efwi_forward_windows)
-against each window run alone through the single-domain path (L1 kernels,
-same launch shape): bitwise identical traces, with and without the CUDA
-graph; receivers outside their window record zeros."""
+"""Shot windows (efwi_forward_windows), in one persistent multi-domain
+launch of the L1-served stencils or as per-window TMA launches on several
+streams, against each window run alone through the single-domain path (L1
+kernels): bitwise identical traces, with and without the CUDA graph;
+receivers outside their window record zeros."""
 import numpy as np
 import pytest
 import torch
@@ -67,6 +68,7 @@ def test_windows_match_single_domain_runs(bx, zchunk, graph):
     from efwi.engine import Propagator
     g, shots, stf, model, windows = _problem()
     P = Propagator(g, tile_bx=bx, zchunk=zchunk)
+    P.set_variant(0)
     P.set_survey(shots, stf)
     P.set_model(*[torch.from_numpy(m) for m in model])
     out = P.forward_windows([0, 1, 2], windows, use_graph=graph).cpu()
@@ -86,3 +88,41 @@ def test_full_grid_window_equals_plain_forward():
     P.set_model(*[torch.from_numpy(m) for m in model])
     full = [(0, 0, g.nx, g.ny)] * 3
     assert torch.equal(P.forward_windows([0, 1, 2], full).cpu(), P.forward([0, 1, 2]).cpu())
+
+
+@pytest.mark.parametrize("cfg,zchunk", [(0, 8), (1, 5), (3, 3)])
+def test_tma_windows_match_single_domain_runs(cfg, zchunk):
+    from efwi.engine import Propagator
+    g, shots, stf, model, windows = _problem()
+    P = Propagator(g, zchunk=zchunk)
+    P.set_variant(1)
+    P.set_tuning(cfg, zchunk, 0, 0)
+    P.set_survey(shots, stf)
+    P.set_model(*[torch.from_numpy(m) for m in model])
+    out = P.forward_windows([0, 1, 2], windows).cpu()
+    parts = P.split(out, [0, 1, 2])
+    for k in range(3):
+        inside, tr = _alone(g, shots[k], stf[k], model, windows[k], 4, zchunk)
+        assert torch.equal(parts[k][:, torch.from_numpy(inside), :], tr)
+        assert float(parts[k][:, torch.from_numpy(~inside), :].abs().max() if (~inside).any() else 0) == 0.0
+
+
+def test_tma_windows_on_eight_streams_equal_the_multi_domain_launch():
+    """11 windows (more than the 8 stream groups; shots repeated on other
+    windows): the per-window TMA launches give the multi-domain launch's
+    bits, receivers of every group included."""
+    from efwi.engine import Propagator
+    g, shots, stf, model, _ = _problem()
+    ids = [0, 0, 0, 1, 1, 1, 2, 2, 2, 0, 1]
+    wins = [(2, 0, 27, 26), (0, 0, 30, 30), (5, 3, 20, 20), (12, 10, 32, 30), (18, 15, 20, 20),
+            (10, 8, 34, 32), (0, 0, 44, 40), (10, 10, 25, 22), (15, 12, 16, 17), (3, 2, 24, 28),
+            (20, 20, 24, 20)]
+    P = Propagator(g, tile_bx=4, zchunk=4)
+    P.set_survey(shots, stf)
+    P.set_model(*[torch.from_numpy(m) for m in model])
+    P.set_variant(0)
+    ref = P.forward_windows(ids, wins, use_graph=True).cpu()
+    P.set_variant(1)
+    out = P.forward_windows(ids, wins).cpu()
+    assert float(ref.abs().max()) > 0
+    assert torch.equal(out, ref)
