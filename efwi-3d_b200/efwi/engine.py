@@ -255,7 +255,8 @@ class Propagator:
 
     def forward_windows(self, shot_ids, windows, use_graph: bool = True) -> torch.Tensor:
         """Traces of shots each on its own window (x0, y0, nx, ny) of the
-        padded grid, all windows in one persistent launch per half-step."""
+        padded grid: per-window TMA launches on several streams (variant 1)
+        or one persistent multi-domain launch per half-step (variant 0)."""
         ids = self._ids(shot_ids)
         if len(windows) != len(ids):
             raise ValueError("one window per shot")

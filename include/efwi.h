@@ -125,11 +125,15 @@ int efwi_gradient(EfwiHandle *h, int n, const int *shot_ids, const float *obs, i
  * window of the padded grid,
  * x in [x0, x0 + nx), y in [y0, y0 + ny), all z, with its own C-PML of npml
  * cells inside the window edges; receivers outside the window record
- * zeros.  All windows of a call advance together in one persistent launch
- * per half-step (L1-served stencils, tile_bx and zchunk of
- * efwi_set_options); use_graph = 1 captures the whole time loop in a CUDA
- * graph and launches it once.  traces: device, concatenation over shot_ids
- * of [3][nrec][nt].  The call synchronises the stream. */
+ * zeros.  With the TMA variant (efwi_set_variant 1, the default) every
+ * window runs the forward TMA kernels as its own grid (forward cfg and
+ * zchunk of efwi_set_tuning), groups of windows on up to 8 internal
+ * streams; use_graph is ignored.  With the L1 variant all windows of a
+ * call advance together in one persistent launch per half-step (tile_bx
+ * and zchunk of efwi_set_options); use_graph = 1 captures the whole time
+ * loop in a CUDA graph and launches it once.  Both give the same bits.
+ * traces: device, concatenation over shot_ids of [3][nrec][nt].  The call
+ * synchronises the stream. */
 typedef struct {
   int x0, y0, nx, ny;
 } EfwiWindow;
