@@ -49,6 +49,8 @@ def parse():
                     help="time steps of the cpu_baseline sample (about 10-30 s of host work)")
     ap.add_argument("--ref-nt", type=int, default=24,
                     help="time steps of each sample of --impl reference (one per step)")
+    ap.add_argument("--lanes", type=int, default=2,
+                    help="shots of the gradient that run concurrently (efwi_set_lanes)")
     ap.add_argument("--tile-bx", type=int, default=4)
     ap.add_argument("--zchunk", type=int, default=8)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
@@ -497,6 +499,7 @@ def main():
     g = prob.grid
     ids = list(range(len(prob.shots)))
     P = Propagator(g, device=dev, tile_bx=a.tile_bx, zchunk=a.zchunk, max_batch=4)
+    P.set_lanes(a.lanes)
     P.set_checkpoint_budget(int(a.ck_budget * (1 << 30)))
     P.set_survey(prob.shots, prob.stf)
     lt, mt, rt = prob.params("true")
@@ -571,6 +574,10 @@ def main():
                 "traffic_source": "ncu capture, one launch (profiles/)" if tr else None,
                 "algorithmic_bytes": kb[dom],
                 "peak_kind": peak_kind, "avg_launch_ms": round(avg_s * 1e3, 4),
+                "lanes": a.lanes if a.mode == "reference" else 1,
+                "note": "with several lanes a launch's events also span the time it shares "
+                        "the GPU with the other lanes' kernels; step_roofline is the whole "
+                        "step" if a.lanes > 1 and a.mode == "reference" else None,
                 "shares": {k: round(v / sum(tot_ms.values()), 4) for k, v in tot_ms.items()}}
     nmodel = (g.nz - 2 * g.npml) * (g.nx - 2 * g.npml) * (g.ny - 2 * g.npml)
     step_bytes = algorithmic_step_bytes(g, nmodel) * g.nt * len(ids)
@@ -582,6 +589,8 @@ def main():
     e2e = None
     if not a.no_e2e and a.mode == "reference":
         import FWI_ops_3d as F
+        P.set_lanes(1)  # frees the extra lanes' workspace for the drop-in's own
+        F.LANES = a.lanes
         with tempfile.TemporaryDirectory() as tmp:
             para = write_dropin_files(tmp, prob, P.split(obs, ids), ids)
             lam_h, mu_h, rho_h = (torch.from_numpy(x).pin_memory() for x in prob.params("init"))
@@ -626,6 +635,7 @@ def main():
                                        f" {len(ids)} shots per GPU, nt={g.nt}, {a.mode} gradient",
                            "model_cells": a.n, "padded": g.nz, "shots_per_gpu": len(ids),
                            "nt": g.nt, "mode": a.mode,
+                           "lanes": a.lanes if a.mode == "reference" else 1,
                            "checkpoints": P.checkpoint_stats() if a.mode == "exact" else None,
                            "l2": "inputs larger than L2 (9 fields x 14 MB per shot + shell store)",
                            "autotune": tune},

@@ -39,6 +39,12 @@ def _mtime(path: str) -> Tuple[float, int]:
     return (st.st_mtime, st.st_size)
 
 
+# Shots of one gradient call that run concurrently on a GPU, each lane with
+# its own workspace and stream (the reference runs them one after another,
+# libCUFD.cu:220-798).
+LANES = 2
+
+
 class _Session:
     """Engine state of one para file on one device."""
 
@@ -68,6 +74,7 @@ class _Session:
             else:
                 self.prop.set_options(if_win=self.para.if_win)
             self.para_key = pk
+        self.prop.set_lanes(LANES)
         sk = (self.para.survey_fname, _mtime(self.para.survey_fname))
         stf_np = stf.detach().to("cpu", torch.float32).contiguous().numpy()
         if sk != self.survey_key or self.stf_cache is None or not np.array_equal(stf_np, self.stf_cache):

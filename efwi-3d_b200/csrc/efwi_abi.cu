@@ -21,6 +21,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/efwi.h"
@@ -56,10 +57,24 @@ const char *kKernelNames[K_NCLASS] = {"stress_fwd", "velocity_fwd", "rev_velocit
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
-  ~DevBuf() { if (p) cudaFree(p); }
+  bool borrowed = false;  // a view of another handle's buffer: never freed here
+  ~DevBuf() { if (p && !borrowed) cudaFree(p); }
+  void view(const DevBuf &o) {
+    if (p && !borrowed) cudaFree(p);
+    p = o.p;
+    bytes = o.bytes;
+    borrowed = true;
+  }
+  void release() {
+    if (p && !borrowed) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    borrowed = false;
+  }
   cudaError_t ensure(size_t n) {
     if (n <= bytes) return cudaSuccess;
-    if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+    if (p && !borrowed) cudaFree(p);
+    p = nullptr; bytes = 0; borrowed = false;
     cudaError_t e = cudaMalloc(&p, n);
     if (e == cudaSuccess) bytes = n;
     return e;
@@ -115,6 +130,12 @@ struct EfwiHandle {
   // shot windows on the TMA kernels: window groups run on their own streams
   cudaStream_t wst[8] = {};
   cudaEvent_t wev[9] = {};
+  // shot lanes of reference-mode calls: sub-handles with their own
+  // workspace and stream, each running a contiguous share of the shots
+  int lanes = 2;
+  std::vector<EfwiHandle *> lane;
+  cudaStream_t own_st = nullptr;  // a lane's stream
+  cudaEvent_t lane_fork = nullptr;
   long long ck_budget = 4LL << 30;  // bytes of checkpoint slots
   long long ck_forward_steps = 0;   // forward steps of the last exact gradient
   // optional outputs of the misfit: windowed synthetics / observed data
@@ -227,6 +248,12 @@ std::vector<int> shell_points(const EfwiGrid &g, int py) {
         if (in) pts.push_back((int)(((long long)z * g.nx + x) * py + y));
       }
   return pts;
+}
+
+__global__ void k_add(float *__restrict__ dst, const float *__restrict__ src, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] += src[i];
 }
 
 __global__ void k_max_vp(const float *lam, const float *mu, const float *rho, long long n,
@@ -955,6 +982,9 @@ void efwi_destroy(EfwiHandle *h) {
     if (s) cudaStreamDestroy(s);
   for (cudaEvent_t e : h->wev)
     if (e) cudaEventDestroy(e);
+  for (EfwiHandle *c : h->lane) efwi_destroy(c);
+  if (h->own_st) cudaStreamDestroy(h->own_st);
+  if (h->lane_fork) cudaEventDestroy(h->lane_fork);
   delete h;
 }
 
@@ -977,6 +1007,17 @@ int efwi_set_tuning(EfwiHandle *h, int fwd_cfg, int zchunk_fwd, int rev_cfg, int
   h->rcfg = rev_cfg;
   if (zchunk_fwd) h->zchunk = zchunk_fwd;
   if (zchunk_rev) h->zchunk_rev = zchunk_rev;
+  return EFWI_OK;
+}
+
+int efwi_set_lanes(EfwiHandle *h, int lanes) {
+  if (!h) return EFWI_ERR_ARG;
+  if (lanes < 1 || lanes > 8) return fail(h, EFWI_ERR_ARG, "lanes must be in [1, 8]");
+  h->lanes = lanes;
+  while ((int)h->lane.size() > lanes - 1) {  // frees the dropped lanes' workspace
+    efwi_destroy(h->lane.back());
+    h->lane.pop_back();
+  }
   return EFWI_OK;
 }
 
@@ -1111,9 +1152,14 @@ int efwi_forward(EfwiHandle *h, int n, const int *ids, float *traces, void *stre
   return status_check(h, st);
 }
 
+// Misfit (and, with glam set, the images) of shots ids on stream st.  With
+// copy_out unset the images stay in the handle's pitched accumulator
+// (h->grad) instead of being copied to glam/gmu/grho; js_out (host, n),
+// when given, receives the misfit of every shot.
 static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs, int mode,
                          double *misfit, float *glam, float *gmu, float *grho, float *res_out,
-                         cudaStream_t st, bool adj_source = false) {
+                         cudaStream_t st, bool adj_source = false, bool copy_out = true,
+                         double *js_out = nullptr) {
   const int nt = h->grid.nt;
   const long long N = h->N;
   const bool grad = glam != nullptr;
@@ -1267,7 +1313,7 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     rc = check_launch(h, "reverse");
     if (rc) return rc;
   }
-  if (grad) {
+  if (grad && copy_out) {
     const EfwiGrid &G = h->grid;
     k_pitch_copy<<<1184, 256, 0, st>>>(glam, out_lam, G.nz, G.nx, G.ny, h->py, 0);
     k_pitch_copy<<<1184, 256, 0, st>>>(gmu, out_mu, G.nz, G.nx, G.ny, h->py, 0);
@@ -1282,6 +1328,7 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
   double J = 0.0;
   for (int k = 0; k < n; ++k) J += js[k];
   if (misfit) *misfit = J;
+  if (js_out) std::copy(js.begin(), js.begin() + n, js_out);
   {
     int rc1 = status_check(h, st);
     if (rc1) return rc1;
@@ -1290,10 +1337,162 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
   return EFWI_OK;
 }
 
+// Copies h's configuration into lane c; c borrows h's model,
+// coefficients, survey and shell points, which no call writes.
+static int lane_sync(EfwiHandle *h, EfwiHandle *c) {
+  c->grid = h->grid;
+  c->geo = h->geo;
+  c->N = h->N;
+  c->py = h->py;
+  c->if_win = h->if_win; c->bx = h->bx; c->zchunk = h->zchunk; c->max_batch = h->max_batch;
+  c->variant = h->variant; c->fcfg = h->fcfg; c->rcfg = h->rcfg; c->zchunk_rev = h->zchunk_rev;
+  c->nt_limit = h->nt_limit;
+  c->prof_sample = h->prof_sample;
+  c->coef.view(h->coef);
+  c->lam.view(h->lam);
+  c->mu.view(h->mu);
+  c->buoy.view(h->buoy);
+  c->model_set = h->model_set;
+  c->shots = h->shots;
+  c->stf.view(h->stf);
+  c->src_cell.view(h->src_cell);
+  c->stf_w2.view(h->stf_w2);
+  c->survey_set = h->survey_set;
+  c->pts.view(h->pts);
+  c->npts = h->npts;
+  c->lanes = 1;
+  if (!c->own_st) CK_CUDA(c, cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking));
+  return EFWI_OK;
+}
+
+// Allocates the large per-shot workspace of a reference-mode call up front;
+// false (with the workspace released and the error cleared) when the GPU
+// has no room for it.
+static bool lane_reserve(EfwiHandle *c, bool grad) {
+  const long long N = c->N;
+  cudaError_t e = c->fields.ensure(sizeof(float) * 9 * N);
+  if (e == cudaSuccess) e = c->psi.ensure(sizeof(float) * psi_per_shot(c->geo));
+  if (grad && e == cudaSuccess) e = c->adj.ensure(sizeof(float) * 9 * N);
+  if (grad && e == cudaSuccess) e = c->grad.ensure(sizeof(float) * 3 * N);
+  if (grad && e == cudaSuccess)
+    e = c->shell.ensure(sizeof(float) * 9 * (size_t)std::max(c->npts, 1) * c->grid.nt);
+  if (e == cudaSuccess) return true;
+  cudaGetLastError();
+  c->fields.release(); c->psi.release(); c->adj.release(); c->grad.release(); c->shell.release();
+  return false;
+}
+
+// Reference-mode misfit / gradient of n >= 2 shots on up to h->lanes
+// lanes: lane 0 is h on the caller's stream, lane l >= 1 a sub-handle with
+// its own workspace and stream, driven by its own host thread.  Lane l
+// takes the contiguous shots [n*l/L, n*(l+1)/L).  Kernels of different
+// lanes share the GPU, which fills the tail waves and launch gaps of one
+// shot's sequence with another shot's work.  The misfit is summed over
+// the shots in order (as with one lane); the images are the lanes'
+// accumulators added in lane order.
+static int gradient_lanes(EfwiHandle *h, int n, const int *ids, const float *obs, double *misfit,
+                          float *glam, float *gmu, float *grho, float *res_out, cudaStream_t st) {
+  const bool grad = glam != nullptr;
+  const int nt = h->grid.nt;
+  int L = std::min(h->lanes, n);
+  if (h->variant == 1) {
+    int rc = get_encoder(h);  // once, before any thread needs it
+    if (rc) return rc;
+  }
+  if (!lane_reserve(h, grad)) L = 1;
+  while ((int)h->lane.size() < L - 1) h->lane.push_back(new EfwiHandle());
+  int got = 1;
+  for (; got < L; ++got) {
+    EfwiHandle *c = h->lane[got - 1];
+    if (lane_sync(h, c)) return fail(h, EFWI_ERR_CUDA, "lane %d: %s", got, c->err.c_str());
+    if (!lane_reserve(c, grad)) break;
+  }
+  L = got;
+  if (L < 2)
+    return gradient_impl(h, n, ids, obs, EFWI_MODE_REFERENCE, misfit, glam, gmu, grho, res_out, st);
+  std::vector<int> b(L + 1);
+  for (int l = 0; l <= L; ++l) b[l] = (int)((long long)n * l / L);
+  std::vector<long long> off(n + 1, 0);
+  for (int k = 0; k < n; ++k) off[k + 1] = off[k] + 3LL * h->shots[ids[k]].nrec * nt;
+  if (!h->lane_fork) CK_CUDA(h, cudaEventCreateWithFlags(&h->lane_fork, cudaEventDisableTiming));
+  CK_CUDA(h, cudaEventRecord(h->lane_fork, st));
+  int dev = 0;
+  CK_CUDA(h, cudaGetDevice(&dev));
+  for (int l = 1; l < L; ++l) {
+    EfwiHandle *c = h->lane[l - 1];
+    const long long o = off[b[l]];
+    c->scr_syn = h->scr_syn ? h->scr_syn + o : nullptr;
+    c->scr_obs = h->scr_obs ? h->scr_obs + o : nullptr;
+    c->scr_res = h->scr_res ? h->scr_res + o : nullptr;
+    CK_CUDA(h, cudaStreamWaitEvent(c->own_st, h->lane_fork, 0));
+  }
+  // No return between the first thread's start and the joins below.
+  std::vector<double> js(n, 0.0);
+  std::vector<int> rcs(L, EFWI_OK);
+  std::vector<std::thread> th;
+  th.reserve(L - 1);
+  auto run_lane = [&](int l) {
+    EfwiHandle *c = h->lane[l - 1];
+    const long long o = off[b[l]];
+    if (cudaSetDevice(dev) != cudaSuccess) {
+      rcs[l] = fail(c, EFWI_ERR_CUDA, "cudaSetDevice(%d) failed in lane %d", dev, l);
+      return;
+    }
+    rcs[l] = gradient_impl(c, b[l + 1] - b[l], ids + b[l], obs + o, EFWI_MODE_REFERENCE, nullptr,
+                           glam, gmu, grho, res_out ? res_out + o : nullptr, c->own_st, false,
+                           false, js.data() + b[l]);
+  };
+  for (int l = 1; l < L; ++l) {
+    try {
+      th.emplace_back(run_lane, l);
+    } catch (...) {
+      run_lane(l);  // no thread to spare: the lane runs here, before lane 0
+    }
+  }
+  rcs[0] = gradient_impl(h, b[1], ids, obs, EFWI_MODE_REFERENCE, nullptr, glam, gmu, grho, res_out,
+                         st, false, false, js.data());
+  for (std::thread &t : th) t.join();
+  for (int l = 1; l < L; ++l) {
+    EfwiHandle *c = h->lane[l - 1];
+    if (h->prof_sample > 0) resolve_profile(c);
+    for (int k = 0; k < K_NCLASS; ++k) {
+      h->launches[k] += c->launches[k];
+      h->timed[k] += c->timed[k];
+      h->ms[k] += c->ms[k];
+      c->launches[k] = 0; c->timed[k] = 0; c->ms[k] = 0;
+    }
+  }
+  for (int l = 0; l < L; ++l)
+    if (rcs[l]) {
+      if (l > 0) h->err = "lane " + std::to_string(l) + ": " + h->lane[l - 1]->err;
+      return rcs[l];
+    }
+  if (grad) {
+    float *acc = h->grad.as<float>();
+    for (int l = 1; l < L; ++l)
+      k_add<<<1184, 256, 0, st>>>(acc, h->lane[l - 1]->grad.as<float>(), 3 * h->N);
+    const EfwiGrid &G = h->grid;
+    k_pitch_copy<<<1184, 256, 0, st>>>(acc, glam, G.nz, G.nx, G.ny, h->py, 0);
+    k_pitch_copy<<<1184, 256, 0, st>>>(acc + h->N, gmu, G.nz, G.nx, G.ny, h->py, 0);
+    k_pitch_copy<<<1184, 256, 0, st>>>(acc + 2 * h->N, grho, G.nz, G.nx, G.ny, h->py, 0);
+    h->launches[K_OTHER] += L - 1 + 3;
+    int rc = check_launch(h, "lane images");
+    if (rc) return rc;
+    CK_CUDA(h, cudaStreamSynchronize(st));
+  }
+  double J = 0.0;
+  for (int k = 0; k < n; ++k) J += js[k];
+  if (misfit) *misfit = J;
+  return EFWI_OK;
+}
+
 int efwi_misfit(EfwiHandle *h, int n, const int *ids, const float *obs, double *misfit, void *stream) {
   int rc = check_ready(h, n, ids);
   if (rc) return rc;
   if (n > 0 && !obs) return fail(h, EFWI_ERR_ARG, "null obs");
+  if (h->lanes > 1 && n > 1)
+    return gradient_lanes(h, n, ids, obs, misfit, nullptr, nullptr, nullptr, nullptr,
+                          (cudaStream_t)stream);
   return gradient_impl(h, n, ids, obs, EFWI_MODE_REFERENCE, misfit, nullptr, nullptr, nullptr,
                        nullptr, (cudaStream_t)stream);
 }
@@ -1306,6 +1505,8 @@ int efwi_gradient(EfwiHandle *h, int n, const int *ids, const float *obs, int mo
   if (!glam || !gmu || !grho) return fail(h, EFWI_ERR_ARG, "null gradient output");
   if (mode != EFWI_MODE_REFERENCE && mode != EFWI_MODE_EXACT)
     return fail(h, EFWI_ERR_ARG, "gradient mode %d is not available", mode);
+  if (mode == EFWI_MODE_REFERENCE && h->lanes > 1 && n > 1)
+    return gradient_lanes(h, n, ids, obs, misfit, glam, gmu, grho, res, (cudaStream_t)stream);
   return gradient_impl(h, n, ids, obs, mode, misfit, glam, gmu, grho, res, (cudaStream_t)stream);
 }
 

@@ -68,6 +68,7 @@ _SIGS = {
     "efwi_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "efwi_set_tuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
     "efwi_set_nt_limit": (C.c_int, [C.c_void_p, C.c_int]),
+    "efwi_set_lanes": (C.c_int, [C.c_void_p, C.c_int]),
     "efwi_set_model": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_set_survey": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(EfwiShot), C.POINTER(C.c_float)]),
     "efwi_forward": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_void_p]),

@@ -119,6 +119,12 @@ class Propagator:
                                                int(rev_cfg), int(zchunk_rev)))
         self.tuning = (fwd_cfg, zchunk_fwd, rev_cfg, zchunk_rev)
 
+    def set_lanes(self, lanes: int) -> None:
+        """Shots of a reference-mode misfit/gradient call that run
+        concurrently, each lane with its own workspace and stream (1-8,
+        default 2; efwi_set_lanes)."""
+        check(self._h, self._L.efwi_set_lanes(self._h, int(lanes)))
+
     def set_nt_limit(self, nt_limit: int) -> None:
         check(self._h, self._L.efwi_set_nt_limit(self._h, int(nt_limit)))
 

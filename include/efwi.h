@@ -82,6 +82,19 @@ int efwi_set_variant(EfwiHandle *h, int variant);
  * No reference counterpart. */
 int efwi_set_tuning(EfwiHandle *h, int fwd_cfg, int zchunk_fwd, int rev_cfg, int zchunk_rev);
 
+/* Shot lanes of reference-mode efwi_misfit / efwi_gradient calls of two or
+ * more shots (replaces the reference's serial shot loop on one GPU,
+ * libCUFD.cu:220-798): lanes in [1, 8], default 2.  Lane 0 runs on the
+ * caller's stream; every further lane has its own workspace (state,
+ * boundary-shell store, images: about 9 floats per boundary-shell cell and
+ * time step plus 21 volumes) and its own stream and host thread, and takes
+ * a contiguous share of the shots, so kernels of different shots share
+ * the GPU.  A lane whose workspace does not fit in device memory is
+ * dropped for the call.  The misfit is identical to one lane; images
+ * differ by the order of the per-shot sums only.  Lowering the count
+ * frees the dropped lanes' workspace.  The call stays synchronous. */
+int efwi_set_lanes(EfwiHandle *h, int lanes);
+
 /* Timing probes: nt_limit > 0 stops the time loops after nt_limit steps
  * (results are then not meaningful); 0 restores the full axis.  No
  * reference counterpart. */
