@@ -301,12 +301,6 @@ k_velocity_fwd_tma(const __grid_constant__ Maps<9> maps, Geo g, Fields f, Psi ps
   }
 }
 
-namespace {
-template <class K>
-void set_smem(K kernel, int bytes) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
-}  // namespace
 
 // Launch configurations of the forward TMA kernels: (TX, ring depth,
 // minimum resident CTAs per SM).  cfg 0-2 use 32 x 4 tiles, cfg 3 32 x 8.
@@ -315,8 +309,8 @@ static void stress_launch(dim3 grid, cudaStream_t st, const Maps<11> &maps, cons
                           const Fields &f, const Psi &ps, int zchunk, int nzc, const SrcArgs &src,
                           int *status) {
   constexpr int B = PlaneRing<3, 8, 2, TX, R>::BYTES;
-  static bool once = (set_smem(k_stress_fwd_tma<TX, R, MINB>, B), true);
-  (void)once;
+  static std::atomic<unsigned long long> smem_set{0};
+  set_smem_once(k_stress_fwd_tma<TX, R, MINB>, B, smem_set);
   k_stress_fwd_tma<TX, R, MINB><<<grid, dim3(32, TX), B, st>>>(maps, g, f, ps, zchunk, nzc, src,
                                                               status);
 }
@@ -325,8 +319,8 @@ template <int TX, int R, int MINB>
 static void velocity_launch(dim3 grid, cudaStream_t st, const Maps<9> &maps, const Geo &g,
                             const Fields &f, const Psi &ps, int zchunk, int nzc, int *status) {
   constexpr int B = PlaneRing<5, 4, 1, TX, R>::BYTES;
-  static bool once = (set_smem(k_velocity_fwd_tma<TX, R, MINB>, B), true);
-  (void)once;
+  static std::atomic<unsigned long long> smem_set{0};
+  set_smem_once(k_velocity_fwd_tma<TX, R, MINB>, B, smem_set);
   k_velocity_fwd_tma<TX, R, MINB><<<grid, dim3(32, TX), B, st>>>(maps, g, f, ps, zchunk, nzc,
                                                                 status);
 }

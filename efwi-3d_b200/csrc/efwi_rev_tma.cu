@@ -419,12 +419,6 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
   }
 }
 
-namespace {
-template <class K>
-void set_smem(K kernel, int bytes) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
-}  // namespace
 
 // Launch configurations of the reverse TMA kernels (32 x 4 tiles):
 // (ring depth, minimum resident CTAs per SM).
@@ -434,8 +428,8 @@ static void revv_launch(dim3 grid, cudaStream_t st, const Maps<K1L<MODE>::N> &ma
                         int nzc, int do_rev, int do_adj, int *status) {
   using L = K1L<MODE>;
   constexpr int B = PlaneRing<L::NH, L::NP, L::NM, 4, R>::BYTES;
-  static bool once = (set_smem(k_rev_velocity_tma<4, R, MINB, MODE>, B), true);
-  (void)once;
+  static std::atomic<unsigned long long> smem_set{0};
+  set_smem_once(k_rev_velocity_tma<4, R, MINB, MODE>, B, smem_set);
   k_rev_velocity_tma<4, R, MINB, MODE><<<grid, dim3(32, 4), B, st>>>(
       maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status);
 }
@@ -446,8 +440,8 @@ static void revs_launch(dim3 grid, cudaStream_t st, const Maps<23> &maps, const 
                         int zchunk, int nzc, int do_rev, int do_adj, const SrcArgs &src,
                         int *status) {
   constexpr int B = PlaneRing<6, 17, 5, 4, R>::BYTES;
-  static bool once = (set_smem(k_rev_stress_tma<4, R, MINB>, B), true);
-  (void)once;
+  static std::atomic<unsigned long long> smem_set{0};
+  set_smem_once(k_rev_stress_tma<4, R, MINB>, B, smem_set);
   k_rev_stress_tma<4, R, MINB><<<grid, dim3(32, 4), B, st>>>(maps, g, f, a, ps, glam, gmu, zchunk,
                                                             nzc, do_rev, do_adj, src, status);
 }

@@ -16,6 +16,8 @@
 #include <cuda.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace efwi {
 
 constexpr int TMA_BOXY = 40;     // y extent of a box (32 + 2 x 4 halo)
@@ -87,6 +89,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 }
 
 // 3-D tiled bulk tensor load of one box into shared memory (no multicast).
+// Raises a kernel's dynamic shared-memory limit once per device: the
+// attribute belongs to the device's context, so a process that drives
+// several GPUs sets it on each (bit d of `done` stands for device d).
+template <class K>
+inline void set_smem_once(K kernel, int bytes, std::atomic<unsigned long long> &done) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  done.fetch_or(bit, std::memory_order_acq_rel);
+}
+
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
                                             int c0, int c1, int c2) {
   asm volatile(
