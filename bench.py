@@ -510,7 +510,10 @@ def main():
     P.set_model(lam, mu, rho)
     from efwi.autotune import autotune
     if a.autotune:
-        tune = autotune(P, 0, P.split(obs, ids)[0].reshape(-1))
+        parts = P.split(obs, ids)
+        pair = (ids[:2], torch.cat([t.reshape(-1) for t in parts[:2]])) if len(ids) >= 2 \
+            else (None, None)
+        tune = autotune(P, 0, parts[0].reshape(-1), pair_ids=pair[0], pair_obs=pair[1])
     else:
         P.set_tuning(*[int(v) for v in a.tuning.split(",")])
         tune = {"fixed": a.tuning}

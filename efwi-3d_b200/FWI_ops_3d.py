@@ -215,8 +215,12 @@ class _FwiOps:
                     obs = s.observed(shards[i])
                     if not s.tuned:
                         # launch shapes timed once per session on the real grid
-                        n0 = 3 * s.shots[shards[i][0]].nrec * s.para.grid.nt
-                        autotune(s.prop, shards[i][0], obs[:n0])
+                        nt = s.para.grid.nt
+                        n0 = 3 * s.shots[shards[i][0]].nrec * nt
+                        two = shards[i][:2] if len(shards[i]) >= 2 else None
+                        n1 = n0 + 3 * s.shots[two[1]].nrec * nt if two else 0
+                        autotune(s.prop, shards[i][0], obs[:n0], pair_ids=two,
+                                 pair_obs=obs[:n1] if two else None)
                         s.tuned = True
                     with _scratch(s, shards[i], obs):
                         results[i] = s.prop.gradient(shards[i], obs)

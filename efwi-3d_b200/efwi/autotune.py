@@ -34,11 +34,32 @@ def _probe(P, shot_ids, obs, names) -> float:
     return t
 
 
+def _time_call(P, ids, obs, reps: int = 2) -> float:
+    """Fastest of `reps` reference-mode gradient calls (ms, CUDA events on
+    the current stream; the call is synchronous, its lanes included)."""
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P.gradient(ids, obs)
+        e1.record()
+        torch.cuda.synchronize(P.device)
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
 def autotune(P, shot_id: int, obs_shot: torch.Tensor, nt_probe: int = 16,
              fwd_cfgs: Sequence[int] = FWD_CFGS, rev_cfgs: Sequence[int] = REV_CFGS,
-             zchunks: Sequence[int] = ZCHUNKS) -> Dict:
+             zchunks: Sequence[int] = ZCHUNKS, pair_ids=None, pair_obs=None,
+             lanes_nt: int = 64) -> Dict:
     """Tunes `P` (a Propagator with model and survey set) on shot `shot_id`
-    whose observed traces are `obs_shot`; returns the timings and the choice."""
+    whose observed traces are `obs_shot`; returns the timings and the choice.
+
+    With two shots `pair_ids` (observed traces `pair_obs`) and more than
+    one lane on P, a last stage times whole two-shot calls, whose lanes
+    share the GPU, for the chosen z planes per CTA and 8 (forward and
+    reverse): concurrent lanes fill each other's tail waves, which favours
+    longer z marches than the kernels timed alone do."""
     ids = [int(shot_id)]
     P.set_nt_limit(nt_probe)
     try:
@@ -58,11 +79,27 @@ def autotune(P, shot_id: int, obs_shot: torch.Tensor, nt_probe: int = 16,
     finally:
         P.set_nt_limit(0)
         P.profile(0)
-    P.set_tuning(bf[0], bf[1], br[0], br[1])
-    return {"fwd_cfg": bf[0], "zchunk_fwd": bf[1], "rev_cfg": br[0], "zchunk_rev": br[1],
-            "fwd_ms": round(fwd[bf], 4), "rev_ms": round(rev[br], 4),
-            "fwd_default_ms": round(fwd.get((0, 8), float("nan")), 4),
-            "rev_default_ms": round(rev.get((0, 8), float("nan")), 4), "probes": len(fwd) + len(rev)}
+    zf, zr = bf[1], br[1]
+    pair = {}
+    if pair_ids is not None and len(pair_ids) >= 2 and getattr(P, "lanes", 1) > 1:
+        P.set_nt_limit(lanes_nt)
+        try:
+            for cand in sorted({(zf, zr), (8, zr), (zf, 8), (8, 8)}):
+                P.set_tuning(bf[0], cand[0], br[0], cand[1])
+                _time_call(P, pair_ids, pair_obs, reps=1)  # warm
+                pair[cand] = _time_call(P, pair_ids, pair_obs)
+        finally:
+            P.set_nt_limit(0)
+        zf, zr = min(pair, key=pair.get)
+    P.set_tuning(bf[0], zf, br[0], zr)
+    out = {"fwd_cfg": bf[0], "zchunk_fwd": zf, "rev_cfg": br[0], "zchunk_rev": zr,
+           "fwd_ms": round(fwd[bf], 4), "rev_ms": round(rev[br], 4),
+           "fwd_default_ms": round(fwd.get((0, 8), float("nan")), 4),
+           "rev_default_ms": round(rev.get((0, 8), float("nan")), 4),
+           "probes": len(fwd) + len(rev) + len(pair)}
+    if pair:
+        out["lanes_probe_ms"] = {f"{a},{b}": round(v, 3) for (a, b), v in pair.items()}
+    return out
 
 
 def autotune_windows(P, shot_ids, windows, nt_probe: int = 16, bxs=(4, 8), zchunks=(4, 8, 16),

@@ -84,6 +84,7 @@ class Propagator:
         check(h, rc)
         self.shots: List[Shot] = []
         self.set_options(if_win=if_win, tile_bx=tile_bx, zchunk=zchunk, max_batch=max_batch)
+        self.lanes = 2  # the engine's default
         self._model_version = None
 
     # ------------------------------------------------------------------ setup
@@ -124,6 +125,7 @@ class Propagator:
         concurrently, each lane with its own workspace and stream (1-8,
         default 2; efwi_set_lanes)."""
         check(self._h, self._L.efwi_set_lanes(self._h, int(lanes)))
+        self.lanes = int(lanes)
 
     def set_nt_limit(self, nt_limit: int) -> None:
         check(self._h, self._L.efwi_set_nt_limit(self._h, int(nt_limit)))

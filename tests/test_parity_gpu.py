@@ -216,8 +216,10 @@ def test_autotuner_keeps_results_and_picks_a_configuration():
     obs = torch.from_numpy(d["B_obs"])
     P = _prop("B_")
     before = P.gradient([0], obs)
-    choice = autotune(P, 0, obs, nt_probe=8, zchunks=(4, 8))
+    choice = autotune(P, 0, obs, nt_probe=8, zchunks=(4, 8),
+                      pair_ids=[0, 0], pair_obs=torch.cat([obs, obs]), lanes_nt=8)
     assert {"fwd_cfg", "rev_cfg", "zchunk_fwd", "zchunk_rev"} <= set(choice)
+    assert len(choice["lanes_probe_ms"]) >= 1
     after = P.gradient([0], obs)
     for x, y in zip(before[1:], after[1:]):
         assert torch.equal(x, y)
