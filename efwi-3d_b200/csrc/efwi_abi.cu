@@ -1347,7 +1347,7 @@ static int lane_sync(EfwiHandle *h, EfwiHandle *c) {
   c->if_win = h->if_win; c->bx = h->bx; c->zchunk = h->zchunk; c->max_batch = h->max_batch;
   c->variant = h->variant; c->fcfg = h->fcfg; c->rcfg = h->rcfg; c->zchunk_rev = h->zchunk_rev;
   c->nt_limit = h->nt_limit;
-  c->prof_sample = h->prof_sample;
+  c->prof_sample = 0;  // lane 0 alone records kernel events (the others count launches)
   c->coef.view(h->coef);
   c->lam.view(h->lam);
   c->mu.view(h->mu);

@@ -91,7 +91,9 @@ int efwi_set_tuning(EfwiHandle *h, int fwd_cfg, int zchunk_fwd, int rev_cfg, int
  * a contiguous share of the shots, so kernels of different shots share
  * the GPU.  A lane whose workspace does not fit in device memory is
  * dropped for the call.  The misfit is identical to one lane; images
- * differ by the order of the per-shot sums only.  Lowering the count
+ * differ by the order of the per-shot sums only.  Kernel events of
+ * efwi_profile are recorded on lane 0 only; launches are counted on all
+ * lanes.  Lowering the count
  * frees the dropped lanes' workspace.  The call stays synchronous. */
 int efwi_set_lanes(EfwiHandle *h, int lanes);
 

@@ -73,7 +73,7 @@ def test_lanes_match_one_lane():
             assert float((a - b).norm() / b.norm()) < 1e-6
         for k in ("stress_fwd", "velocity_fwd", "rev_velocity", "rev_stress", "misfit"):
             assert prof[k]["launches"] == prof1[k]["launches"], k
-            assert prof[k]["timed"] == prof1[k]["timed"], k
+            assert 0 < prof[k]["timed"] <= prof1[k]["timed"], k  # lane 0 alone is timed
     P.close()
 
 
