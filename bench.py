@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--pair-n", type=int, default=40, help="inversion case: model cells of a pair")
     ap.add_argument("--pair-nt", type=int, default=500)
     ap.add_argument("--nprobe", type=int, default=4)
+    ap.add_argument("--net-mode", default="step", choices=["step", "h0"],
+                    help="inversion case: the CNN's direction tried first ('step') or the CNN "
+                         "as the initial inverse Hessian of L-BFGS ('h0')")
     ap.add_argument("--epochs", type=int, default=20)
     return ap.parse_args()
 
@@ -322,10 +325,11 @@ def run_inversion(a):
     obj = VpObjective(prob, mode=a.mode)
     vp0 = torch.from_numpy(prob.vp_init).cuda()
     plain = lbfgs(obj, vp0, iters=a.iters, log=log)
-    learned = lbfgs(obj, vp0, iters=a.iters, net=net, stop_misfit=plain.misfit[-1], log=log)
+    learned = lbfgs(obj, vp0, iters=a.iters, net=net, stop_misfit=plain.misfit[-1], log=log,
+                    net_mode=a.net_mode)
     target = plain.misfit[-1]
     t_learned = next((t for t, j in zip(learned.seconds, learned.misfit) if j <= target), None)
-    line = {"case": "inversion", "problem": prob.name, "mode": a.mode,
+    line = {"case": "inversion", "problem": prob.name, "mode": a.mode, "net_mode": a.net_mode,
             "plain": {"misfit": plain.misfit, "seconds": plain.seconds,
                       "model_rel_l2": plain.model_rel_l2, "evals": plain.evals},
             "learned": {"misfit": learned.misfit, "seconds": learned.seconds,

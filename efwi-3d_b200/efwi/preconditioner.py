@@ -9,11 +9,17 @@
   probing estimator of Bekas, Kokiopoulou & Saad (2007) applied to J^T J.
 * The CNN (efwi.cnn.Preconditioner, BF16 tensor-core convolutions) maps the
   cheap inputs to the expensive direction.
-* L-BFGS with the learned step: each iteration first tries the CNN's
-  direction under a backtracking Armijo line search; if the line search
-  rejects it, the plain L-BFGS direction is used (and is itself line
-  searched).  The curvature pairs of accepted steps feed the L-BFGS memory
-  either way.  The plain method is the same loop without the CNN.
+* L-BFGS with the learned step (net_mode "step"): each iteration first
+  tries the CNN's direction under a backtracking Armijo line search; if the
+  line search rejects it, the plain L-BFGS direction is used (and is itself
+  line searched).  The curvature pairs of accepted steps feed the L-BFGS
+  memory either way.  The plain method is the same loop without the CNN.
+* net_mode "h0": the CNN, made homogeneous in its gradient input, is the
+  initial inverse Hessian of the two-loop recursion (Nocedal & Wright 2006,
+  Algorithm 7.4, with H0 = gamma N instead of gamma I; gamma = s'y / y'N(y)
+  along the newest pair), so the learned map preconditions the quasi-Newton
+  step instead of replacing it; the identity-H0 direction is the fallback
+  when the line search rejects the preconditioned one.
 
 The model is vp on the model grid; vs and rho stay at their initial values,
 as in the reference's inversion drivers, which update vp only
@@ -227,10 +233,16 @@ class LbfgsResult:
     evals: int
 
 
+def _sync(dev) -> None:
+    if torch.device(dev).type == "cuda":
+        torch.cuda.synchronize(dev)
+
+
 def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10,
           net=None, first_step: float = 20.0, c1: float = 1e-4, max_trials: int = 12,
           max_expand: int = 3, learned_trials: int = 4,
-          stop_misfit: Optional[float] = None, bounds=(1000.0, 6000.0), log=None) -> LbfgsResult:
+          stop_misfit: Optional[float] = None, bounds=(1000.0, 6000.0), log=None,
+          net_mode: str = "step") -> LbfgsResult:
     """L-BFGS on vp with an Armijo line search -- backtracking by halves, or
     doubling (up to max_expand times) while the misfit keeps falling when
     the unit step is accepted at once; trial points cost a forward
@@ -240,8 +252,14 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
     `learned_trials` halvings); the plain L-BFGS direction is the fallback
     when that line search fails.  `first_step`
     (m/s) scales the first plain step, like the reference's Adam learning
-    rate of 20 m/s (3D_inversion_adam.py)."""
-    torch.cuda.synchronize(obj.dev)
+    rate of 20 m/s (3D_inversion_adam.py).
+
+    net_mode "h0" uses `net` as the initial inverse Hessian of the two-loop
+    recursion instead (module docstring); `learned_accepted` then counts the
+    iterations whose preconditioned direction was accepted."""
+    if net_mode not in ("step", "h0"):
+        raise ValueError(f"net_mode must be 'step' or 'h0', not {net_mode!r}")
+    _sync(obj.dev)
     t0 = time.perf_counter()
     vp = vp0.clone()
     J, g = obj.value_and_grad(vp)
@@ -250,7 +268,13 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
     last_dmax = first_step
     illum = obj.illumination(vp) if net is not None else None
 
-    def two_loop(q):
+    def learned_map(q):
+        """The CNN applied to q as a gradient, scaled back by q's largest
+        entry, so that N(c q) = c N(q) for c > 0."""
+        with torch.no_grad():
+            return net(features(q, vp, illum)).to(q.dtype) * q.abs().max()
+
+    def two_loop(q, h0=None):
         q = q.clone()
         al = []
         for s, y in reversed(list(zip(S, Y))):
@@ -258,7 +282,16 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
             a = rho * torch.sum(s * q)
             q -= a * y
             al.append((rho, a))
-        if S:
+        if h0 is not None:
+            nq = h0(q)
+            if S:
+                yn = torch.sum(Y[-1] * h0(Y[-1]))
+                if not float(yn) > 0:
+                    return None  # the map is not positive along y: no learned H0
+                r = (torch.sum(S[-1] * Y[-1]) / yn) * nq
+            else:
+                r = nq * (first_step / (nq.abs().max() + 1e-30))
+        elif S:
             gamma = torch.sum(S[-1] * Y[-1]) / torch.sum(Y[-1] * Y[-1])
             r = gamma * q
         else:
@@ -292,7 +325,12 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
 
     for it in range(iters):
         step = None
-        if net is not None:
+        if net is not None and net_mode == "h0":
+            d = two_loop(g, learned_map)
+            step = search(d, J, g, max_trials) if d is not None else None
+            if step is not None:
+                res.learned_accepted += 1
+        elif net is not None:
             with torch.no_grad():
                 dl = -net(features(g, vp, illum))
             dl = dl * (last_dmax / (dl.abs().max() + 1e-30))
@@ -313,7 +351,7 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
                 Y.pop(0)
         last_dmax = float(s.abs().max())
         vp, J, g = vn, Jn, gn
-        torch.cuda.synchronize(obj.dev)
+        _sync(obj.dev)
         res.misfit.append(J)
         res.seconds.append(time.perf_counter() - t0)
         res.model_rel_l2.append(_rel(vp, obj.vp_true))
