@@ -42,9 +42,14 @@ def parse():
     ap.add_argument("--nt", type=int, default=2000)
     ap.add_argument("--shots", type=int, default=16)
     ap.add_argument("--n", type=int, default=128, help="model cells per axis")
-    ap.add_argument("--profile-sample", type=int, default=64,
-                    help="time every k-th step's launches with CUDA events (the events "
-                         "cost about 10 %% of the step at k = 8 with two lanes)")
+    ap.add_argument("--profile-sample", type=int, default=16,
+                    help="untimed profiling pass: time every k-th time step's launches "
+                         "with CUDA events")
+    ap.add_argument("--profile-shots", type=int, default=2,
+                    help="shots of the untimed one-lane profiling pass")
+    ap.add_argument("--parity-nt", type=int, default=160,
+                    help="time steps of the parity sample (1 shot of the grid, against "
+                         "the reference's kernels and the FP64 port on the host)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nt", type=int, default=160,
@@ -176,8 +181,8 @@ def kernel_bytes(grid, nshot_launch=1):
 
 # DRAM bytes (read + write) per launch of the stencil kernels on the 152^3
 # padded grid (128^3 model, C-PML 12), one shot per launch, from one ncu
-# capture each (profiles/stencil_rev_tma_config2.md,
-# profiles/stencil_fwd_tma_config2.md); other grids report no traffic.
+# capture of each kernel (dram__bytes_read.sum + dram__bytes_write.sum);
+# other grids report no traffic.
 TRAFFIC_152 = {"rev_velocity": 415.4e6, "rev_stress": 501.3e6,
                "stress_fwd": 221.6e6, "velocity_fwd": 184.4e6}
 
@@ -220,6 +225,68 @@ class CpuSample:
     @property
     def cores(self):
         return self.lib.num_threads()
+
+
+def profile_pass(P, ids, obs_all, mode, sample):
+    """Per-kernel CUDA-event times of one gradient over `ids` on one lane,
+    every `sample`-th time step (untimed; restores the lane count)."""
+    lanes = P.lanes
+    P.set_lanes(1)
+    parts = P.split(obs_all, list(range(len(P.shots))))
+    import torch
+    obs = torch.cat([parts[k].reshape(-1) for k in ids])
+    P.profile(sample)
+    P.profile_read()
+    P.gradient(ids, obs, mode=mode)
+    torch.cuda.synchronize()
+    prof = P.profile_read()
+    P.profile(0)
+    P.set_lanes(lanes)
+    return prof
+
+
+def parity_sample(a, dev):
+    """Rel-L2 of this engine against the reference's own kernels (oracle/_ref,
+    FP32 on the host) and the FP64 port, on one shot of the benchmark grid
+    with a short time axis: traces of the true model, then the misfit and
+    the reference-mode gradient of the initial model against those traces."""
+    import numpy as np
+    import torch
+    import oracle
+    from efwi import synthetic
+    from efwi.engine import Propagator
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import case_of, rel_l2
+    p = synthetic.config2(nt=a.parity_nt, nshot=1, n=a.n)
+    P = Propagator(p.grid, device=dev)
+    P.set_survey(p.shots, p.stf)
+    P.set_model(*[torch.from_numpy(x) for x in p.params("true")])
+    tr = P.forward([0])
+    P.set_model(*[torch.from_numpy(x) for x in p.params("init")])
+    J, gl, gm, gr = P.gradient([0], tr)
+    ours = [x.cpu().numpy() for x in (gl, gm, gr)]
+    tr_np = tr.cpu().numpy()
+    P.close()
+    out = {"sample": f"1 shot of config 2's {p.grid.nz}^3 padded grid, nt={a.parity_nt}; "
+                     "observed data = this engine's true-model traces for all three",
+           "tolerance": {"traces_vs_reference_kernels": 1e-5, "vs_fp64_port": 1e-4}}
+    t0 = time.perf_counter()
+    legs = []
+    if oracle.ref_available():
+        legs.append(("reference_kernels", oracle.ref(), np.float32))
+    legs.append(("fp64_port", oracle.port(), np.float64))
+    for name, lib, dt in legs:
+        rtr = lib.forward(case_of(p, "true", dt))[0]
+        obs = [tr_np.reshape(3, -1, a.parity_nt).astype(dt)]
+        if name == "fp64_port":
+            Jr, rl, rm, rr, _ = lib.gradient(case_of(p, "init", dt), obs, mode=0)
+        else:
+            Jr, rl, rm, rr, _ = lib.gradient(case_of(p, "init", dt), obs)
+        out["vs_" + name] = {"traces": rel_l2(tr_np, rtr), "misfit": abs(J - Jr) / abs(Jr),
+                             "g_lambda": rel_l2(ours[0], rl), "g_mu": rel_l2(ours[1], rm),
+                             "g_rho": rel_l2(ours[2], rr)}
+    out["host_seconds"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def run_reference(a):
@@ -525,13 +592,16 @@ def main():
         tune = {"fixed": a.tuning}
 
     stream = torch.cuda.current_stream(dev)
+    # the three images and the misfit of a step, summed over ranks with one
+    # all-reduce (efwi.dist.ShotParallel does the same for library users)
+    from efwi.dist import pack_misfit
+    stacked = torch.empty(3 * g.ncell + 2, dtype=torch.float32, device=dev)
 
     def step():
-        J, gl, gm, gr = P.gradient(ids, obs, mode=a.mode)
+        J, gl, gm, gr = P.gradient(ids, obs, mode=a.mode, out=stacked)
         if world > 1:
-            jt = torch.tensor([J], device=dev, dtype=torch.float32)
-            for t in (gl, gm, gr, jt):
-                dist.all_reduce(t)
+            pack_misfit(stacked, J)
+            dist.all_reduce(stacked)
         return gl
 
     for _ in range(a.warmup):
@@ -541,7 +611,8 @@ def main():
         dist.barrier()
     clk = Clocks(local)
     clk.start()
-    P.profile(a.profile_sample)
+    # The timed region runs with kernel events off; launches are counted.
+    P.profile(0)
     P.profile_read()  # reset counters
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -554,9 +625,14 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    prof = P.profile_read()
-    P.profile(0)
+    counted = P.profile_read()
     clocks = clk.stop()
+    # Per-kernel launch times from a separate, untimed pass on one lane (no
+    # other shot's kernels share the GPU with the timed launches): every
+    # k-th time step of a gradient over the first shots.
+    prof = profile_pass(P, ids[:a.profile_shots], obs, a.mode, a.profile_sample)
+    for k in prof:
+        prof[k]["launches"] = counted.get(k, {}).get("launches", 0)
     ms_local = e0.elapsed_time(e1) / a.steps
     ms = ms_local
     if world > 1:
@@ -565,7 +641,7 @@ def main():
         ms = float(t.item())
     cells_step = prob.cell_steps * world
     value = cells_step / (ms * 1e-3) / 1e9
-    launches = int(sum(v["launches"] for v in prof.values()))
+    launches = int(sum(v["launches"] for v in counted.values()))
 
     # roofline of the dominant kernel (share of timed launches)
     peak, peak_kind = peaks()
@@ -580,13 +656,12 @@ def main():
         tr = TRAFFIC_152.get(dom) if (g.nz, g.nx, g.ny, g.npml) == (152, 152, 152, 12) else None
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": tr,
-                "traffic_source": "ncu capture, one launch (profiles/)" if tr else None,
+                "traffic_source": "ncu capture, one launch" if tr else None,
                 "algorithmic_bytes": kb[dom],
                 "peak_kind": peak_kind, "avg_launch_ms": round(avg_s * 1e3, 4),
-                "lanes": a.lanes if a.mode == "reference" else 1,
-                "note": "with several lanes a launch's events also span the time it shares "
-                        "the GPU with the other lanes' kernels; step_roofline is the whole "
-                        "step" if a.lanes > 1 and a.mode == "reference" else None,
+                "timing": f"CUDA events on one lane (no concurrent shots), every "
+                          f"{a.profile_sample}th time step of a gradient over "
+                          f"{len(ids[:a.profile_shots])} shots, outside the timed region",
                 "shares": {k: round(v / sum(tot_ms.values()), 4) for k, v in tot_ms.items()}}
     nmodel = (g.nz - 2 * g.npml) * (g.nx - 2 * g.npml) * (g.ny - 2 * g.npml)
     step_bytes = algorithmic_step_bytes(g, nmodel) * g.nt * len(ids)
@@ -627,6 +702,10 @@ def main():
                    "h2d_bytes_per_step": 3 * nb, "d2h_bytes_per_step": 3 * nb + 4,
                    "ms_per_step": ms_e2e, "api": "FWI_ops_3d.fwi_ops.backward (host tensors)"}
 
+    parity = None
+    if rank == 0 and world == 1 and not a.no_cpu and a.parity_nt > 0:
+        parity = parity_sample(a, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cs = CpuSample("port", a.n, a.cpu_nt)
@@ -649,6 +728,7 @@ def main():
                            "l2": "inputs larger than L2 (9 fields x 14 MB per shot + shell store)",
                            "autotune": tune},
                 "roofline": roof, "step_roofline": whole, "cpu_baseline": cpu, "e2e": e2e,
+                "parity": parity,
                 "gpu_launches": launches, "clocks": clocks,
                 "kernel_profile": {k: {"launches": v["launches"],
                                        "avg_ms": (v["ms"] / v["timed"]) if v["timed"] else None}

@@ -144,6 +144,31 @@ def _shards(ids: List[int], ngpu: int) -> List[List[int]]:
     return [ids[cut[i]:cut[i + 1]] for i in range(ngpu)]
 
 
+def _reduce_shards(results, dev):
+    """Sum of the per-GPU (misfit, gλ, gμ, gρ) of the shards in shard order
+    (Torch_Fwi.cpp:89-94 adds them on the host).  The images are summed on
+    the first shard's device, each other shard's three volumes arriving in
+    one peer copy, and the sum then moves to `dev` once; the misfit is
+    summed in float32 as the reference's host loop does."""
+    J = np.float32(0.0)
+    for r in results:
+        J += np.float32(r[0])
+    base = results[0][1].device
+    n = results[0][1].numel()
+    shape = results[0][1].shape
+    acc = torch.empty(3 * n, dtype=torch.float32, device=base)
+    for k in range(3):
+        acc[k * n:(k + 1) * n].copy_(results[0][1 + k].reshape(-1))
+    if len(results) > 1:
+        part = torch.empty_like(acc)
+        for r in results[1:]:
+            for k in range(3):
+                part[k * n:(k + 1) * n].copy_(r[1 + k].reshape(-1), non_blocking=True)
+            acc += part
+    out = acc.to(dev)
+    return float(J), *(out[k * n:(k + 1) * n].view(shape) for k in range(3))
+
+
 class _scratch:
     """scratch_dir_name (Parameter.cpp:118-124): after the misfit, writes
     Residual_Shot_{x,y,z}{id}.bin, Syn_Shot_... and CondObs_Shot_... --
@@ -240,16 +265,7 @@ class _FwiOps:
             if e is not None:
                 raise e
         dev = Lambda.device if isinstance(Lambda, torch.Tensor) else torch.device("cpu")
-        gl = torch.zeros(Lambda.shape, dtype=torch.float32, device=dev)
-        gm = torch.zeros_like(gl)
-        gr = torch.zeros_like(gl)
-        J = 0.0
-        for i in range(ngpu):
-            Ji, a, b, c = results[i]
-            gl += a.to(dev)
-            gm += b.to(dev)
-            gr += c.to(dev)
-            J += np.float32(Ji)
+        J, gl, gm, gr = _reduce_shards(results, dev)
         gstf = torch.zeros(torch.as_tensor(stf).shape, dtype=torch.float32, device=dev)
         return [torch.tensor([J], dtype=torch.float32), gl, gm, gr, gstf]
 

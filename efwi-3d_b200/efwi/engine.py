@@ -216,8 +216,13 @@ class Propagator:
         return J.value
 
     def gradient(self, shot_ids, obs: torch.Tensor, mode: str = "reference",
-                 want_residual: bool = False):
-        """Misfit and gradients w.r.t. lambda, mu, rho (device tensors)."""
+                 want_residual: bool = False, out: Optional[torch.Tensor] = None):
+        """Misfit and gradients w.r.t. lambda, mu, rho (device tensors).
+
+        `out`, if given, is a contiguous float32 device tensor of at least
+        3 * nz * nx * ny elements: the three images are written into it one
+        after the other (and returned as views), so that a caller can sum
+        them over ranks with one collective."""
         ids = self._ids(shot_ids)
         obs = _f32_dev(obs, self.device)
         if self.shots and all(0 <= k < len(self.shots) for k in ids) and \
@@ -225,7 +230,17 @@ class Propagator:
             raise ValueError("observed data size does not match the shots")
         m = {"reference": _lib.MODE_REFERENCE, "exact": _lib.MODE_EXACT}[mode]
         shp = self.grid.shape
-        gl, gm, gr = (torch.empty(shp, device=self.device, dtype=torch.float32) for _ in range(3))
+        if out is not None:
+            n = self.grid.ncell
+            if (out.dtype != torch.float32 or out.device != self.device
+                    or not out.is_contiguous() or out.numel() < 3 * n):
+                raise ValueError("out must be a contiguous float32 tensor of >= 3 volumes "
+                                 "on the engine's device")
+            flat = out.view(-1)
+            gl, gm, gr = (flat[k * n:(k + 1) * n].view(shp) for k in range(3))
+        else:
+            gl, gm, gr = (torch.empty(shp, device=self.device, dtype=torch.float32)
+                          for _ in range(3))
         res = torch.empty_like(obs) if want_residual else None
         J = C.c_double(0.0)
         with torch.cuda.device(self.device):

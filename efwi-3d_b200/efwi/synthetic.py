@@ -166,3 +166,13 @@ def small(nz=26, nx=30, ny=28, npml=6, nt=120, nshot=1, nrec=12, seed=0, dt=1e-3
     return Problem("small", grid, shots, stf, vp_true.astype(np.float32), vs.astype(np.float32),
                    rho.astype(np.float32), vp.astype(np.float32), vs.astype(np.float32),
                    rho.astype(np.float32))
+
+
+def config3(nt: Optional[int] = None, nshot: int = 4, seed: int = 3) -> Problem:
+    """96^3 model (120^3 padded with a 12-cell C-PML), 4 shots, nt 4000: the
+    differentiation and checkpointing configuration.  It names no spacing,
+    time step or wavelet; those of config 2 are used (dx 10 m, dt 0.8 ms,
+    8 Hz Ricker, random layers and anomalies, smoothed initial model)."""
+    p = config2(nt=nt or 4000, nshot=nshot, seed=seed, n=96)
+    p.name = "config3: 96^3, %d shots, nt=%d" % (len(p.shots), p.grid.nt)
+    return p

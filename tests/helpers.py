@@ -73,3 +73,30 @@ def fixture_engine(prefix: str):
             sh.src_weight = float(d[prefix + "src_weight"][k])
         shots.append(sh)
     return g, shots, d[prefix + "stf"], d[prefix + "lam"], d[prefix + "mu"], d[prefix + "rho"]
+
+
+# (axis, C-PML slot) of state components 9..26, the oracle's order
+PSI_AXIS_SLOT = [(0, 0), (1, 1), (2, 1), (0, 1), (1, 0), (2, 2), (0, 2), (1, 2), (2, 0),
+                 (0, 3), (1, 3), (2, 3), (0, 4), (1, 4), (1, 5), (2, 5), (2, 4), (0, 5)]
+
+
+def step_support(g):
+    """Cells the step updates: fields on [2, n-3]^3; memory variables there
+    and inside their slab (x/y velocity-stage slabs with quirk Q2)."""
+    nz, nx, ny, np_ = g.nz, g.nx, g.ny, g.npml
+    z = np.arange(nz)[:, None, None]
+    x = np.arange(nx)[None, :, None]
+    y = np.arange(ny)[None, None, :]
+    inner = (z >= 2) & (z <= nz - 3) & (x >= 2) & (x <= nx - 3) & (y >= 2) & (y <= ny - 3)
+    coords = (z, x, y)
+    ns = (nz, nx, ny)
+    m = np.zeros((27, nz, nx, ny), bool)
+    m[:9] = inner
+    for k, (ax, slot) in enumerate(PSI_AXIS_SLOT):
+        c, n = coords[ax], ns[ax]
+        if slot >= 3 and ax > 0:
+            slab = (c < np_) | (c > n - np_)
+        else:
+            slab = (c < np_) | (c > n - np_ - 1)
+        m[9 + k] = inner & slab
+    return m

@@ -16,14 +16,9 @@ import pytest
 import torch
 
 import oracle
-from helpers import case_of, rel_l2
+from helpers import PSI_AXIS_SLOT, case_of, rel_l2, step_support as _support
 
 pytestmark = pytest.mark.gpu
-
-# (axis, C-PML slot) of state components 9..26, the oracle's order
-PSI_AXIS_SLOT = [(0, 0), (1, 1), (2, 1), (0, 1), (1, 0), (2, 2), (0, 2), (1, 2), (2, 0),
-                 (0, 3), (1, 3), (2, 3), (0, 4), (1, 4), (1, 5), (2, 5), (2, 4), (0, 5)]
-
 
 @pytest.fixture(scope="module", autouse=True)
 def _ready():
@@ -39,28 +34,6 @@ def _engine(p, which="init", **opts):
     lam, mu, rho = p.params(which)
     P.set_model(torch.from_numpy(lam), torch.from_numpy(mu), torch.from_numpy(rho))
     return P
-
-
-def _support(g):
-    """Cells the step updates: fields on [2, n-3]^3; memory variables there
-    and inside their slab (x/y velocity-stage slabs with quirk Q2)."""
-    nz, nx, ny, np_ = g.nz, g.nx, g.ny, g.npml
-    z = np.arange(nz)[:, None, None]
-    x = np.arange(nx)[None, :, None]
-    y = np.arange(ny)[None, None, :]
-    inner = (z >= 2) & (z <= nz - 3) & (x >= 2) & (x <= nx - 3) & (y >= 2) & (y <= ny - 3)
-    coords = (z, x, y)
-    ns = (nz, nx, ny)
-    m = np.zeros((27, nz, nx, ny), bool)
-    m[:9] = inner
-    for k, (ax, slot) in enumerate(PSI_AXIS_SLOT):
-        c, n = coords[ax], ns[ax]
-        if slot >= 3 and ax > 0:
-            slab = (c < np_) | (c > n - np_)
-        else:
-            slab = (c < np_) | (c > n - np_ - 1)
-        m[9 + k] = inner & slab
-    return m
 
 
 def _small(seed=1):
