@@ -31,7 +31,7 @@ from efwi import config as _cfg
 from efwi.autotune import autotune
 from efwi.engine import Propagator
 
-__all__ = ["fwi_ops", "FWIFunction", "FWI_3d", "FWI_obscalc"]
+__all__ = ["fwi_ops", "FWIFunction", "FWI_3d", "FWI_obscalc", "set_lanes"]
 
 
 def _mtime(path: str) -> Tuple[float, int]:
@@ -41,8 +41,26 @@ def _mtime(path: str) -> Tuple[float, int]:
 
 # Shots of one gradient call that run concurrently on a GPU, each lane with
 # its own workspace and stream (the reference runs them one after another,
-# libCUFD.cu:220-798).
+# libCUFD.cu:220-798).  A lane beyond the first holds its own state (about
+# 21 volumes) and boundary-shell store (9 floats per shell point and time
+# step: 37.6 GB at 152^3 and nt 2000) outside torch's allocator.  Set with
+# set_lanes(n) or FWI_3d(..., opt={"lanes": n}); a lane that does not fit in
+# device memory at the call is left out.
 LANES = 2
+_lanes_by_para: Dict[str, int] = {}
+
+
+def set_lanes(n: int, para_fname: Optional[str] = None) -> None:
+    """Concurrent shots of later gradient calls: for every para file, or
+    (para_fname given) for that one."""
+    n = int(n)
+    if not 1 <= n <= 8:
+        raise ValueError("lanes must be in [1, 8]")
+    global LANES
+    if para_fname is None:
+        LANES = n
+    else:
+        _lanes_by_para[os.path.abspath(para_fname)] = n
 
 
 class _Session:
@@ -74,7 +92,7 @@ class _Session:
             else:
                 self.prop.set_options(if_win=self.para.if_win)
             self.para_key = pk
-        self.prop.set_lanes(LANES)
+        self.prop.set_lanes(_lanes_by_para.get(self.para_fname, LANES))
         sk = (self.para.survey_fname, _mtime(self.para.survey_fname))
         stf_np = stf.detach().to("cpu", torch.float32).contiguous().numpy()
         if sk != self.survey_key or self.stf_cache is None or not np.array_equal(stf_np, self.stf_cache):
@@ -351,6 +369,8 @@ class FWI_3d(torch.nn.Module):
             self.Mask = Mask
         self.Stf = Stf
         self.para_fname = opt['para_fname']
+        if 'lanes' in opt:
+            set_lanes(opt['lanes'], self.para_fname)
 
     def forward(self, Shot_ids, ngpu=1):
         Vp_pad, Vs_pad, Rho_pad = ft.padding_3d(self.Vp, self.Vs, self.Rho, self.nz, self.nx,

@@ -26,6 +26,7 @@
 
 #include "../../include/efwi.h"
 #include "efwi_exact.h"
+#include "efwi_fuse.cuh"
 #include "efwi_kernels.h"
 #include "efwi_revolve.h"
 
@@ -95,6 +96,48 @@ struct Pending {
   cudaEvent_t a, b;
 };
 
+// CUDA graph of one time loop, replayed while the launch parameters the
+// loop bakes in (buffer addresses, tensor maps, tuning, time axis: the key)
+// are unchanged -- across the shots of a call and across calls.
+struct GraphCache {
+  std::string key;
+  cudaGraphExec_t exec = nullptr;
+  long long launches[K_NCLASS] = {0};  // kernel launches of one replay, by class
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    key.clear();
+  }
+  ~GraphCache() { reset(); }
+};
+
+// Byte image of the values that make up a graph's key: scalars, pointers
+// and padding-free structs (Fields, Psi, tensor maps) as they are; the
+// structs with padding field by field.
+struct KeyBytes {
+  std::string s;
+  template <class T>
+  KeyBytes &add(const T &v) {
+    s.append(reinterpret_cast<const char *>(&v), sizeof(T));
+    return *this;
+  }
+  KeyBytes &rec(const RecArgs &r) {
+    // the fused kernels read no count, only whether there are receivers
+    const int n = r.plane ? (r.ncell > 0) : r.ncell;
+    return add(r.ucell).add(r.ushot).add(r.uptr).add(r.rec).add(r.trace_off).add(r.nrec).add(n)
+        .add(r.plane).add(r.map).add(r.nxpy);
+  }
+  KeyBytes &src(const SrcArgs &a) { return add(a.cell).add(a.stf).add(a.nt); }
+  KeyBytes &shell(const ShellMap &m) {
+    return add(m.rows).add(m.store).add(m.npts).add(m.ya0).add(m.ya1).add(m.yb0).add(m.yb1);
+  }
+  KeyBytes &geo(const Geo &g) {
+    return add(g.nz).add(g.nx).add(g.ny).add(g.np).add(g.N).add(g.sz).add(g.sx).add(g.dt)
+        .add(g.idz).add(g.idx).add(g.idy).add(g.slab_z).add(g.slab_x).add(g.slab_y).add(g.cz)
+        .add(g.cx).add(g.cy);
+  }
+};
+
 }  // namespace
 
 struct EfwiHandle {
@@ -118,6 +161,12 @@ struct EfwiHandle {
 
   DevBuf pts;
   int npts = 0;
+  // row table of the shell points for the save/restore fused into the TMA
+  // stencil kernels (efwi_fuse.cuh); shell_fused false: separate kernels
+  DevBuf shell_rows;
+  ShellMap shm{};
+  bool shell_fused = false;
+  DevBuf recmap;  // per-plane receiver maps of the current batch
 
   DevBuf fields, psi, adj, traces_tm, res_tm, shell, partial, jdev, recbuf, winbuf, scalar, grad;
   DevBuf status;  // pipeline status word (EFWI_STATUS_*)
@@ -145,6 +194,11 @@ struct EfwiHandle {
   DevBuf stf_w2;  // taper factor w^2 of the source-time functions [nt]
   DevBuf scr_tm;
   int ck_slots = 0;                 // slots it used
+
+  // time loops of reference-mode gradients and forward batches as CUDA
+  // graphs (efwi_set_graphs; kernel-event sampling runs them eagerly)
+  bool use_graphs = true;
+  GraphCache g_fwd, g_rev;
 
   int prof_sample = 0;
   std::vector<cudaEvent_t> ev_pool;
@@ -250,6 +304,49 @@ std::vector<int> shell_points(const EfwiGrid &g, int py) {
   return pts;
 }
 
+// Row table of the shell points (efwi_fuse.cuh): for every row (z, x) the
+// index of its first point, with SHELL_SPLIT set when the row holds the two
+// runs [ya0, ya1] and [yb0, yb1] instead of the one run [ya0, yb1].  Checked
+// against the list point by point (a bijection between the cells the table
+// names and the points); false when the points do not have that form.
+bool shell_rows(const EfwiGrid &g, int py, const std::vector<int> &pts, std::vector<int> *rows,
+                ShellMap *m) {
+  rows->assign((size_t)g.nz * g.nx, -1);
+  const int lo = g.npml - 2, hy = g.ny - g.npml + 1;
+  m->ya0 = std::max(lo, 2);
+  m->yb1 = std::min(hy, g.ny - 3);
+  m->ya1 = std::min(lo + 4, m->yb1);
+  m->yb0 = std::max(hy - 4, m->ya0);
+  const bool can_split = m->ya1 + 1 < m->yb0;
+  const long long nsplit = (m->ya1 - m->ya0 + 1) + (m->yb1 - m->yb0 + 1);
+  m->npts = (int)pts.size();
+  if (pts.size() >= (size_t)SHELL_SPLIT) return false;
+  size_t k = 0;
+  while (k < pts.size()) {
+    const int zx = pts[k] / py;
+    size_t e = k;
+    while (e < pts.size() && pts[e] / py == zx) ++e;
+    const long long cnt = (long long)(e - k);
+    if (pts[k] % py != m->ya0) return false;
+    if (cnt == m->yb1 - m->ya0 + 1) (*rows)[zx] = (int)k;
+    else if (can_split && cnt == nsplit) (*rows)[zx] = (int)k | SHELL_SPLIT;
+    else return false;
+    k = e;
+  }
+  long long named = 0;
+  for (long long zx = 0; zx < (long long)g.nz * g.nx; ++zx) {
+    const int row = (*rows)[zx];
+    if (row < 0) continue;
+    for (int y = 0; y < g.ny; ++y) {
+      const int q = shell_index(*m, row, y);
+      if (q < 0) continue;
+      if (q >= (int)pts.size() || pts[q] != (int)(zx * py + y)) return false;
+      ++named;
+    }
+  }
+  return named == (long long)pts.size();
+}
+
 __global__ void k_add(float *__restrict__ dst, const float *__restrict__ src, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -297,6 +394,46 @@ struct Timer {
 int check_launch(EfwiHandle *h, const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(h, EFWI_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
+  return EFWI_OK;
+}
+
+// Runs `body(stream)` -- a time loop of kernel launches with no host
+// synchronisation -- through the graph cache `gc`: replays the cached graph
+// when its key matches, otherwise captures body on the handle's capture
+// stream, instantiates it and replays it.  Launches are counted per replay.
+// Eager (body on st) when graphs are off or kernel events are sampled.
+template <class Body>
+int run_graphed(EfwiHandle *h, GraphCache &gc, const std::string &key, cudaStream_t st,
+                Body body) {
+  if (!h->use_graphs || h->prof_sample > 0) return body(st);
+  if (!h->cap_stream) CK_CUDA(h, cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+  if (!gc.exec || gc.key != key) {
+    gc.reset();
+    long long before[K_NCLASS];
+    std::memcpy(before, h->launches, sizeof(before));
+    cudaGraph_t graph = nullptr;
+    CK_CUDA(h, cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body(h->cap_stream);
+    cudaError_t ec = cudaStreamEndCapture(h->cap_stream, &graph);
+    for (int k = 0; k < K_NCLASS; ++k) {
+      gc.launches[k] = h->launches[k] - before[k];
+      h->launches[k] = before[k];
+    }
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      return rc;
+    }
+    if (ec == cudaSuccess) ec = cudaGraphInstantiate(&gc.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (ec != cudaSuccess) {
+      gc.reset();
+      return fail(h, EFWI_ERR_CUDA, "graph of a time loop: %s", cudaGetErrorString(ec));
+    }
+    gc.key = key;
+  }
+  CK_CUDA(h, cudaGraphLaunch(gc.exec, st));
+  for (int k = 0; k < K_NCLASS; ++k) h->launches[k] += gc.launches[k];
   return EFWI_OK;
 }
 
@@ -432,6 +569,38 @@ int upload_receivers(EfwiHandle *h, const RecHost &r, cudaStream_t st, RecArgs *
   out->rec = (const int *)(p + b0 + b1 + b2 + b3);
   out->nrec = (const int *)(p + b0 + b1 + b2 + b3 + b4);
   out->ncell = (int)r.ucell.size();
+  // Per-plane maps of the unique receiver cells for the gather / injection
+  // fused into the TMA stencil kernels; none for the L1 kernels, or when
+  // the receivers spread over so many planes that the maps would pass
+  // 64 Mi cells (the separate kernels run then).
+  out->plane = nullptr;
+  out->map = nullptr;
+  const int nz = h->grid.nz;
+  const long long nxpy = (long long)h->grid.nx * h->py;
+  out->nxpy = (int)nxpy;
+  const int S = (int)r.trace_off.size();
+  if (h->variant == 1 && !r.ucell.empty()) {
+    std::vector<int> plane((size_t)S * nz, -1);
+    int nmaps = 0;
+    for (size_t u = 0; u < r.ucell.size(); ++u) {
+      int &m = plane[(size_t)r.ushot[u] * nz + (int)(r.ucell[u] / nxpy)];
+      if (m < 0) m = nmaps++;
+    }
+    if ((long long)nmaps * nxpy <= (64LL << 20)) {
+      std::vector<int> maps((size_t)nmaps * nxpy, -1);
+      for (size_t u = 0; u < r.ucell.size(); ++u) {
+        const int m = plane[(size_t)r.ushot[u] * nz + (int)(r.ucell[u] / nxpy)];
+        maps[(size_t)m * nxpy + (size_t)(r.ucell[u] % nxpy)] = (int)u;
+      }
+      const size_t pb = al(plane.size() * 4);
+      CK_CUDA(h, h->recmap.ensure(pb + maps.size() * 4));
+      char *q = h->recmap.as<char>();
+      CK_CUDA(h, cudaMemcpyAsync(q, plane.data(), plane.size() * 4, cudaMemcpyHostToDevice, st));
+      CK_CUDA(h, cudaMemcpyAsync(q + pb, maps.data(), maps.size() * 4, cudaMemcpyHostToDevice, st));
+      out->plane = (const int *)q;
+      out->map = (const int *)(q + pb);
+    }
+  }
   return EFWI_OK;
 }
 
@@ -456,16 +625,35 @@ int nt_eff(const EfwiHandle *h) {
 }
 
 // One forward time step of a batch: stress (+ source), velocity, receivers.
+// With `shell` set (one shot), the boundary shell of the step's starting
+// state is stored there first.  On the TMA kernels the shell store and the
+// receiver gather run in the stencil kernels' epilogues; otherwise as
+// separate launches.
 int forward_step(EfwiHandle *h, Fields f, Psi ps, int S, const SrcArgs &src, const RecArgs &rec,
-                 float *traces_tm, cudaStream_t st, int it, const FwdMaps *maps) {
+                 float *traces_tm, cudaStream_t st, int it, const FwdMaps *maps,
+                 float *shell = nullptr) {
   int nzc;
   const int bx = maps ? fwd_tma_tile(h->fcfg) : h->bx;
   const dim3 grid = stencil_grid(h, S, bx, h->zchunk, &nzc);
   int *status = h->status.as<int>();
+  ShellMap shm{};
+  if (shell && h->npts > 0) {
+    if (maps && h->shell_fused) {
+      shm = h->shm;
+      shm.store = shell;
+    } else {
+      Timer t(h, K_SHELL_SAVE, st, it);
+      k_shell_save<<<(h->npts + 255) / 256, 256, 0, st>>>(f, h->pts.as<int>(), h->npts, shell);
+    }
+  }
+  RecFuse rf{};
+  const bool rec_fused = maps && rec.ncell > 0 && rec.plane;
+  if (rec_fused) rf = RecFuse{rec, traces_tm, it + 1};
   {
     Timer t(h, K_STRESS_FWD, st, it);
     if (maps)
-      launch_stress_fwd_tma(h->fcfg, grid, st, maps->s, h->geo, f, ps, h->zchunk, nzc, src, status);
+      launch_stress_fwd_tma(h->fcfg, grid, st, maps->s, h->geo, f, ps, h->zchunk, nzc, src, shm,
+                            status);
     else
       launch_stress_fwd(h->bx, grid, st, h->geo, f, ps, h->lam.as<float>(), h->mu.as<float>(),
                         h->zchunk, nzc, src);
@@ -473,11 +661,12 @@ int forward_step(EfwiHandle *h, Fields f, Psi ps, int S, const SrcArgs &src, con
   {
     Timer t(h, K_VELOCITY_FWD, st, it);
     if (maps)
-      launch_velocity_fwd_tma(h->fcfg, grid, st, maps->v, h->geo, f, ps, h->zchunk, nzc, status);
+      launch_velocity_fwd_tma(h->fcfg, grid, st, maps->v, h->geo, f, ps, h->zchunk, nzc, rf,
+                              status);
     else
       launch_velocity_fwd(h->bx, grid, st, h->geo, f, ps, h->buoy.as<float>(), h->zchunk, nzc);
   }
-  if (rec.ncell > 0) {
+  if (rec.ncell > 0 && !rec_fused) {
     Timer t(h, K_RECORD, st, it);
     k_record<<<(rec.ncell + 127) / 128, 128, 0, st>>>(f, h->N, rec, traces_tm, it + 1);
   }
@@ -560,17 +749,22 @@ int run_forward_batch(EfwiHandle *h, const int *ids, int S, float *traces_tm, lo
   if (rec_out) *rec_out = b.rec;
   const int npts = h->npts;
   const int ntl = nt_eff(h);
-  for (int it = 0; it <= ntl - 2; ++it) {
-    if (shell) {
-      Timer t(h, K_SHELL_SAVE, st, it);
-      k_shell_save<<<(npts + 255) / 256, 256, 0, st>>>(b.f, h->pts.as<int>(), npts,
-                                                       shell + (size_t)it * 9 * npts);
+  auto loop = [&](cudaStream_t s) -> int {
+    for (int it = 0; it <= ntl - 2; ++it) {
+      b.src.it = it;
+      const int r = forward_step(h, b.f, b.ps, S, b.src, b.rec, traces_tm, s, it, b.mp,
+                                 shell ? shell + (size_t)it * 9 * npts : nullptr);
+      if (r) return r;
     }
-    b.src.it = it;
-    rc = forward_step(h, b.f, b.ps, S, b.src, b.rec, traces_tm, st, it, b.mp);
-    if (rc) return rc;
-  }
-  return check_launch(h, "forward");
+    return check_launch(h, "forward");
+  };
+  KeyBytes key;
+  key.add(b.f).add(b.ps).rec(b.rec).src(b.src).add(S).add(ntl).add(traces_tm).add(shell)
+      .add(npts).add(h->fcfg).add(h->zchunk).add(h->bx).add(h->variant).geo(h->geo)
+      .shell(h->shm).add(h->shell_fused).add(h->status.p).add(h->lam.p).add(h->mu.p)
+      .add(h->buoy.p);
+  if (b.mp) key.add(b.maps);
+  return run_graphed(h, h->g_fwd, key.s, st, loop);
 }
 
 int resolve_profile(EfwiHandle *h) {
@@ -708,6 +902,21 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
   const int zc = h->zchunk_rev;
   const int bxe = h->bx;
   const dim3 grid = stencil_grid(h, 1, bxe, zc, &nzc);
+  // adjoint kernels with bulk-copy staged planes (TMA variant): tensor maps
+  // over this shot's buffers
+  const bool etma = h->variant == 1 && (bxe == 4 || bxe == 8);
+  Maps<11> mes;
+  Maps<10> mev;
+  if (etma) {
+    const float *hs[11] = {a.szz, a.sxx, a.syy, a.sxz, a.sxy, a.syz, h->lam.as<float>(),
+                           h->mu.as<float>(), b.f.vz, b.f.vx, b.f.vy};
+    const float *hv[10] = {a.vz, a.vx, a.vy, h->buoy.as<float>(), b.f.sxz, b.f.sxx, b.f.sxy,
+                           b.f.syz, b.f.syy, b.f.szz};
+    for (int k2 = 0; k2 < 11 && rc == 0; ++k2) rc = make_map(h, &mes.m[k2], hs[k2], 1, true, bxe);
+    for (int k2 = 0; k2 < 10 && rc == 0; ++k2) rc = make_map(h, &mev.m[k2], hv[k2], 1, true, bxe);
+    if (rc) return rc;
+  }
+  int *status = h->status.as<int>();
   int par_s = 0, par_v = 0;
   bool first = true;
   for (const CkAction &act : plan.actions) {
@@ -763,7 +972,9 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
       }
       if (k <= ntl - 2) {
         Timer t(h, K_ADJ_STRESS, st, k);
-        launch_adj_stress_exact(bxe, grid, st, exact_args(h, b.f, b.ps, a, par_s, glam, gmu), zc, nzc);
+        const ExactArgs A = exact_args(h, b.f, b.ps, a, par_s, glam, gmu);
+        if (etma) launch_adj_stress_tma(bxe, grid, st, mes, A, zc, status);
+        else launch_adj_stress_exact(bxe, grid, st, A, zc, nzc);
         par_s ^= 1;
       }
       if (k >= 1) {
@@ -773,7 +984,9 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
                                                               adj_source ? 1.0f : -2.0f);
         }
         Timer t(h, K_ADJ_VELOCITY, st, k);
-        launch_adj_velocity_exact(bxe, grid, st, exact_args(h, b.f, b.ps, a, par_v, gB, nullptr), zc, nzc);
+        const ExactArgs A = exact_args(h, b.f, b.ps, a, par_v, gB, nullptr);
+        if (etma) launch_adj_velocity_tma(bxe, grid, st, mev, A, zc, status);
+        else launch_adj_velocity_exact(bxe, grid, st, A, zc, nzc);
         par_v ^= 1;
       }
     }
@@ -879,9 +1092,9 @@ int window_loop_tma(EfwiHandle *h, const std::vector<Domain> &dom, const std::ve
         const Domain &d = dom[k];
         const SrcArgs src{dsrc + k, d.stf, nt, it};
         launch_stress_fwd_tma(h->fcfg, grids[k], s, maps[k].s, d.g, d.f, d.ps, h->zchunk, nzcs[k],
-                              src, status);
+                              src, ShellMap{}, status);
         launch_velocity_fwd_tma(h->fcfg, grids[k], s, maps[k].v, d.g, d.f, d.ps, h->zchunk,
-                                nzcs[k], status);
+                                nzcs[k], RecFuse{}, status);
       }
       const int r0 = rstart[gbeg[g]], r1 = rstart[gbeg[g + 1]];
       if (r1 > r0) {
@@ -970,6 +1183,14 @@ int efwi_create(const EfwiGrid *g, EfwiHandle **out) {
   if (!pts.empty()) {
     CK_CUDA(h, h->pts.ensure(sizeof(int) * pts.size()));
     CK_CUDA(h, cudaMemcpy(h->pts.p, pts.data(), sizeof(int) * pts.size(), cudaMemcpyHostToDevice));
+    std::vector<int> rows;
+    h->shell_fused = shell_rows(*g, h->py, pts, &rows, &h->shm);
+    if (h->shell_fused) {
+      CK_CUDA(h, h->shell_rows.ensure(sizeof(int) * rows.size()));
+      CK_CUDA(h, cudaMemcpy(h->shell_rows.p, rows.data(), sizeof(int) * rows.size(),
+                            cudaMemcpyHostToDevice));
+      h->shm.rows = h->shell_rows.as<int>();
+    }
   }
   return EFWI_OK;
 }
@@ -1024,6 +1245,16 @@ int efwi_set_lanes(EfwiHandle *h, int lanes) {
 int efwi_set_nt_limit(EfwiHandle *h, int nt_limit) {
   if (!h || nt_limit < 0) return EFWI_ERR_ARG;
   h->nt_limit = nt_limit;
+  return EFWI_OK;
+}
+
+int efwi_set_graphs(EfwiHandle *h, int on) {
+  if (!h) return EFWI_ERR_ARG;
+  h->use_graphs = on != 0;
+  if (!h->use_graphs) {
+    h->g_fwd.reset();
+    h->g_rev.reset();
+  }
   return EFWI_OK;
 }
 
@@ -1235,7 +1466,7 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
     Maps<23> m2;
     Maps<13> m1r;
     Maps<12> m1a;
-    const bool split = h->rcfg >= 6;
+    const bool split = h->rcfg == 6 || h->rcfg == 7;
     const bool tma = h->variant == 1;
     const EfwiGrid &G = h->grid;
     if (tma) {
@@ -1246,8 +1477,9 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
       const float *p2[17] = {f.szz, f.sxx, f.syy, f.sxz, f.sxy, f.syz, a.szz, a.sxx, a.syy,
                              a.sxz, a.sxy, a.syz, h->lam.as<float>(), h->mu.as<float>(),
                              h->buoy.as<float>(), glam, gmu};
+      const int bxm = rev_tma_tile(h->rcfg);
       for (int k2 = 0; k2 < 21 && rc == 0; ++k2)
-        rc = make_map(h, &m1.m[k2], k2 < 11 ? h1[k2] : p1[k2 - 11], 1, k2 < 11, 4);
+        rc = make_map(h, &m1.m[k2], k2 < 11 ? h1[k2] : p1[k2 - 11], 1, k2 < 11, bxm);
       if (split) {
         const float *r1[13] = {f.sxz, f.syz, f.sxx, f.sxy, f.syy, f.vz, f.vx, f.vy,
                                a.vz, a.vx, a.vy, h->buoy.as<float>(), grho};
@@ -1257,23 +1489,38 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
         for (int k2 = 0; k2 < 12 && rc == 0; ++k2) rc = make_map(h, &m1a.m[k2], a1[k2], 1, k2 < 6, 4);
       }
       for (int k2 = 0; k2 < 23 && rc == 0; ++k2)
-        rc = make_map(h, &m2.m[k2], k2 < 6 ? h2[k2] : p2[k2 - 6], 1, k2 < 6, 4);
+        rc = make_map(h, &m2.m[k2], k2 < 6 ? h2[k2] : p2[k2 - 6], 1, k2 < 6, bxm);
       if (rc) return rc;
     }
     int nzc;
-    const int bxr = tma ? 4 : h->bx;
+    const int bxr = tma ? rev_tma_tile(h->rcfg) : h->bx;
     const int zcr = tma ? h->zchunk_rev : h->zchunk;
     const dim3 grid = stencil_grid(h, 1, bxr, zcr, &nzc);
     (void)G;
     int *status = h->status.as<int>();
+    // On the TMA kernels the shell restore and the adjoint-source injection
+    // run in K1's and K2's epilogues; otherwise as separate launches.
+    const bool shell_fused = tma && h->shell_fused && npts > 0;
+    const bool inj_fused = tma && rec.ncell > 0 && rec.plane;
+    auto shell_at = [&](int rev, int it) {
+      ShellMap m{};
+      if (shell_fused && rev) {
+        m = h->shm;
+        m.store = const_cast<float *>(shell) + (size_t)it * 9 * npts;
+      }
+      return m;
+    };
     auto K1 = [&](int rev, int adj, int it) {
       Timer t(h, K_REV_VELOCITY, st, it);
+      const ShellMap sm = shell_at(rev, it);
+      RecFuse inj{};
+      if (inj_fused && adj) inj = RecFuse{rec, h->res_tm.as<float>(), it};
       if (tma && split)
         launch_rev_velocity_split_tma(h->rcfg, grid, st, m1r, m1a, h->geo, f, a, ps, grho, zcr,
-                                      nzc, rev, adj, status);
+                                      nzc, rev, adj, sm, inj, status);
       else if (tma)
         launch_rev_velocity_tma(h->rcfg, grid, st, m1, h->geo, f, a, ps, grho, zcr, nzc, rev, adj,
-                                status);
+                                sm, inj, status);
       else
         launch_rev_velocity(h->bx, grid, st, h->geo, f, a, ps, h->lam.as<float>(),
                             h->mu.as<float>(), h->buoy.as<float>(), grho, zcr, nzc, rev, adj);
@@ -1283,34 +1530,47 @@ static int gradient_impl(EfwiHandle *h, int n, const int *ids, const float *obs,
       src.it = it;
       if (tma)
         launch_rev_stress_tma(h->rcfg, grid, st, m2, h->geo, f, a, ps, glam, gmu, zcr, nzc, rev,
-                              adj, src, status);
+                              adj, src, shell_at(rev, it), status);
       else
         launch_rev_stress(h->bx, grid, st, h->geo, f, a, ps, h->lam.as<float>(), h->mu.as<float>(),
                           h->buoy.as<float>(), glam, gmu, zcr, nzc, rev, adj, src);
     };
     auto inject = [&](int it) {
-      if (rec.ncell == 0) return;
+      if (rec.ncell == 0 || inj_fused) return;
       Timer t(h, K_INJECT, st, it);
       k_inject<<<(rec.ncell + 127) / 128, 128, 0, st>>>(a, N, rec, h->res_tm.as<float>(), it, 1.0f);
     };
     auto restore = [&](int it, int stress) {
-      if (npts == 0) return;
+      if (npts == 0 || shell_fused) return;
       Timer t(h, K_SHELL_RESTORE, st, it);
       k_shell_restore<<<(npts + 255) / 256, 256, 0, st>>>(f, h->pts.as<int>(), npts, shell + (size_t)it * 9 * npts, stress);
     };
     const int ntl = nt_eff(h);
-    K1(0, 1, ntl - 1);
-    inject(ntl - 1);
-    K2(0, 1, ntl - 1);
-    for (int it = ntl - 2; it >= 0; --it) {
-      const int adj = it > 0;  // the adjoint update of step 0 feeds no image
-      K1(1, adj, it);
-      if (adj) inject(it);
-      restore(it, 0);
-      K2(1, adj, it);
-      restore(it, 1);
-    }
-    rc = check_launch(h, "reverse");
+    auto loop = [&](cudaStream_t s) -> int {
+      st = s;  // the launch helpers above use st
+      K1(0, 1, ntl - 1);
+      inject(ntl - 1);
+      K2(0, 1, ntl - 1);
+      for (int it = ntl - 2; it >= 0; --it) {
+        const int adj = it > 0;  // the adjoint update of step 0 feeds no image
+        K1(1, adj, it);
+        if (adj) inject(it);
+        restore(it, 0);
+        K2(1, adj, it);
+        restore(it, 1);
+      }
+      return check_launch(h, "reverse");
+    };
+    KeyBytes key;
+    key.add(f).add(a).add(ps).add(grho).add(glam).add(gmu).add(shell).add(npts).rec(rec)
+        .src(src).add(h->res_tm.p).add(h->rcfg).add(zcr).add(bxr).add(h->bx).add(tma)
+        .add(split).add(shell_fused).add(inj_fused).add(ntl).geo(h->geo).shell(h->shm)
+        .add(h->status.p).add(h->lam.p).add(h->mu.p).add(h->buoy.p);
+    if (tma) key.add(m1).add(m2);
+    if (tma && split) key.add(m1r).add(m1a);
+    cudaStream_t caller = st;
+    rc = run_graphed(h, h->g_rev, key.s, caller, loop);
+    st = caller;
     if (rc) return rc;
   }
   if (grad && copy_out) {
@@ -1347,6 +1607,7 @@ static int lane_sync(EfwiHandle *h, EfwiHandle *c) {
   c->if_win = h->if_win; c->bx = h->bx; c->zchunk = h->zchunk; c->max_batch = h->max_batch;
   c->variant = h->variant; c->fcfg = h->fcfg; c->rcfg = h->rcfg; c->zchunk_rev = h->zchunk_rev;
   c->nt_limit = h->nt_limit;
+  c->use_graphs = h->use_graphs;
   c->prof_sample = 0;  // lane 0 alone records kernel events (the others count launches)
   c->coef.view(h->coef);
   c->lam.view(h->lam);
@@ -1360,6 +1621,9 @@ static int lane_sync(EfwiHandle *h, EfwiHandle *c) {
   c->survey_set = h->survey_set;
   c->pts.view(h->pts);
   c->npts = h->npts;
+  c->shell_rows.view(h->shell_rows);
+  c->shm = h->shm;
+  c->shell_fused = h->shell_fused;
   c->lanes = 1;
   if (!c->own_st) CK_CUDA(c, cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking));
   return EFWI_OK;
@@ -1464,6 +1728,12 @@ static int gradient_lanes(EfwiHandle *h, int n, const int *ids, const float *obs
   }
   for (int l = 0; l < L; ++l)
     if (rcs[l]) {
+      // A failed lane may have returned with kernels still queued on its
+      // stream (and the others keep running): drain every lane's stream
+      // before the workspaces can be freed or reused.
+      cudaStreamSynchronize(st);
+      for (int m = 1; m < L; ++m) cudaStreamSynchronize(h->lane[m - 1]->own_st);
+      cudaGetLastError();
       if (l > 0) h->err = "lane " + std::to_string(l) + ": " + h->lane[l - 1]->err;
       return rcs[l];
     }

@@ -38,6 +38,7 @@
 // issued before the plane's one barrier.
 #include "efwi_common.cuh"
 #include "efwi_exact.h"
+#include "efwi_tma.cuh"
 
 namespace efwi {
 namespace {
@@ -73,17 +74,22 @@ struct GS {
   float ez, ex, ey, xz, xy, yz;
 };
 
-__device__ __forceinline__ GS gs_at(const ExactArgs &A, int n) {
-  const float l = A.lam[n], u = A.mu[n], l2u = l + 2.0f * u, dt = A.g.dt;
-  const float azz = A.a.szz[n], axx = A.a.sxx[n], ayy = A.a.syy[n];
+__device__ __forceinline__ GS gs_from(float l, float u, float azz, float axx, float ayy, float axz,
+                                      float axy, float ayz, float dt) {
+  const float l2u = l + 2.0f * u;
   GS r;
   r.ez = (l2u * azz + l * (axx + ayy)) * dt;
   r.ex = (l2u * axx + l * (azz + ayy)) * dt;
   r.ey = (l2u * ayy + l * (azz + axx)) * dt;
-  r.xz = u * A.a.sxz[n] * dt;
-  r.xy = u * A.a.sxy[n] * dt;
-  r.yz = u * A.a.syz[n] * dt;
+  r.xz = u * axz * dt;
+  r.xy = u * axy * dt;
+  r.yz = u * ayz * dt;
   return r;
+}
+
+__device__ __forceinline__ GS gs_at(const ExactArgs &A, int n) {
+  return gs_from(A.lam[n], A.mu[n], A.a.szz[n], A.a.sxx[n], A.a.syy[n], A.a.sxz[n], A.a.sxy[n],
+                 A.a.syz[n], A.g.dt);
 }
 
 // Q of the z-axis terms of the stress stage at (zn, x, y):
@@ -628,6 +634,545 @@ __global__ void __launch_bounds__(32 * BX) k_adj_velocity_exact(ExactArgs A, int
   }
 }
 
+
+// ------------------------------------------------ bulk-copy staged variants
+// The same transposes with every plane's operands staged by bulk tensor
+// copies (efwi_tma.cuh) into a ring of R plane slots of halo boxes,
+// 40 (y) x (TX + 4) (x): the inputs of G and the forward fields of the
+// images.  The CTA's ring runs over planes z0-2 .. z1+1; computing plane z
+// reads the slot of z (x/y neighbours, own cell) and the centres of z+1 and
+// z+2 (the z-stencil queue heads), so three slots stay resident and R-3
+// are in flight.  The Q of the tile and its halo are formed from the slot
+// (the kernels above form the halo's from global loads), the operands of the
+// read-modify-writes are loaded before the ring wait, and the per-cell
+// arithmetic is the same expression as above, so results are bitwise equal.
+
+// Slot fields of the stress-stage transpose.
+enum { ES_ZZ = 0, ES_XX, ES_YY, ES_XZ, ES_XY, ES_YZ, ES_L, ES_M, ES_VZ, ES_VX, ES_VY, ES_N };
+// Slot fields of the velocity-stage transpose.
+enum { EV_VZ = 0, EV_VX, EV_VY, EV_B, EV_SXZ, EV_SXX, EV_SXY, EV_SYZ, EV_SYY, EV_SZZ, EV_N };
+
+template <class Ring>
+__device__ __forceinline__ GS gs_slot(const Ring &ring, int j, int o, float dt) {
+  return gs_from(ring.halo(j, ES_L)[o], ring.halo(j, ES_M)[o], ring.halo(j, ES_ZZ)[o],
+                 ring.halo(j, ES_XX)[o], ring.halo(j, ES_YY)[o], ring.halo(j, ES_XZ)[o],
+                 ring.halo(j, ES_XY)[o], ring.halo(j, ES_YZ)[o], dt);
+}
+
+// Q of the z-axis terms of the stress stage at plane zn from G (qs_z).
+__device__ __forceinline__ void qs_z_of(const ExactArgs &A, const GS &G, int zn, int x, int y,
+                                        float &qez, float &qvx, float &qvy) {
+  const Geo &g = A.g;
+  if (zn < 2 || zn > g.nz - 3) { qez = qvx = qvy = 0.f; return; }
+  if (slab_s(zn, g.nz, g.np)) {
+    const int k = psi32_z(g, zn, x, y);
+    const float *c = g.cz;
+    const int nz = g.nz;
+    qez = qpml(G.ez, true, A.lin.z[PSI_VA * (int)g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+    qvx = qpml(G.xz, true, A.lin.z[PSI_VB1 * (int)g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+    qvy = qpml(G.yz, true, A.lin.z[PSI_VB2 * (int)g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+  } else {
+    qez = G.ez; qvx = G.xz; qvy = G.yz;
+  }
+}
+
+// x-axis terms at row xn from G (qs_x).
+__device__ __forceinline__ void qs_x_of(const ExactArgs &A, const GS &G, int z, int xn, int y,
+                                        float &qex, float &qvz, float &qvy) {
+  const Geo &g = A.g;
+  if (xn < 2 || xn > g.nx - 3) { qex = qvz = qvy = 0.f; return; }
+  if (slab_s(xn, g.nx, g.np)) {
+    const int k = psi32_x(g, z, xn, y);
+    const float *c = g.cx;
+    const int nx = g.nx;
+    qex = qpml(G.ex, true, A.lin.x[PSI_VA * (int)g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+    qvz = qpml(G.xz, true, A.lin.x[PSI_VB1 * (int)g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+    qvy = qpml(G.xy, true, A.lin.x[PSI_VB2 * (int)g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+  } else {
+    qex = G.ex; qvz = G.xz; qvy = G.xy;
+  }
+}
+
+// y-axis terms at column yn from G (qs_y).
+__device__ __forceinline__ void qs_y_of(const ExactArgs &A, const GS &G, int z, int x, int yn,
+                                        float &qey, float &qvz, float &qvx) {
+  const Geo &g = A.g;
+  if (yn < 2 || yn > g.ny - 3) { qey = qvz = qvx = 0.f; return; }
+  if (slab_s(yn, g.ny, g.np)) {
+    const int k = psi32_y(g, z, x, yn);
+    const float *c = g.cy;
+    const int ny = g.ny;
+    qey = qpml(G.ey, true, A.lin.y[PSI_VA * (int)g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qvz = qpml(G.yz, true, A.lin.y[PSI_VB1 * (int)g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+    qvx = qpml(G.xy, true, A.lin.y[PSI_VB2 * (int)g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+  } else {
+    qey = G.ey; qvz = G.yz; qvx = G.xy;
+  }
+}
+
+template <int TX, int R, int MINB>
+__global__ void __launch_bounds__(32 * TX, MINB)
+k_adj_stress_tma(const __grid_constant__ Maps<ES_N> maps, ExactArgs A, int zchunk, int *status) {
+  using Ring = PlaneRing<ES_N, 0, 0, TX, R>;
+  __shared__ float sqx[3][TX + 4][32];
+  __shared__ float sqy[3][TX][36];
+  extern __shared__ __align__(128) unsigned char smem[];
+  Ring ring;
+  ring.bind(smem);
+  const Geo &g = A.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int y0 = blockIdx.x * 32, x0 = blockIdx.y * TX;
+  const int y = y0 + tx, x = x0 + ty;
+  const int z0 = max((int)blockIdx.z * zchunk, 2);
+  const int z1 = min((int)blockIdx.z * zchunk + zchunk, g.nz - 2);
+  if (z0 >= z1) return;  // uniform over the CTA, before any barrier
+  const int nq = z1 - z0, nj = nq + 4;  // ring planes z0-2 .. z1+1
+  if (tid == 0) ring.init();
+  __syncthreads();
+  if (tid == 0)
+    for (int j = 0; j < nj && j < R; ++j) ring.issue(maps, j, y0, x0, z0 - 2 + j, z0 - 2 + j);
+
+  const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
+  const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
+  const bool xin = x >= 2 && x <= nx - 3, yin = y >= 2 && y <= ny - 3;
+  const bool act = xin && yin;
+  const bool xs = slab_s(x, nx, np), ys = slab_s(y, ny, np);
+  // halo roles: rows 0, 1, TX+2, TX+3 of sqx (threads ty < 4) and columns
+  // 0, 1, 34, 35 of sqy (threads tx < 4)
+  const int hr = ty < 2 ? ty : TX + ty;
+  const int hxn = x0 - 2 + hr;
+  const int hc = tx < 2 ? tx : 32 + tx;
+  const int hyn = y0 - 2 + hc;
+  const int own = (ty + TMA_HX) * TMA_BOXY + tx + TMA_HY;  // own cell in a box
+  const int hro = hr * TMA_BOXY + tx + TMA_HY;             // halo row cell
+  const int hco = (ty + TMA_HX) * TMA_BOXY + hc + 2;       // halo column cell
+
+  bool ok = true;
+  for (int j = 0; j < 4; ++j) ok = ring.wait(j) && ok;
+  // queues: Q_z of planes z-2 .. z+2 (head z+2 per plane); forward vz at
+  // z-2 .. z+1, vx and vy at z-1 .. z+2 (heads z+1 and z+2 per plane)
+  float qez[5] = {}, qvx[5] = {}, qvy[5] = {};
+  float zvz[4] = {}, zvx[4] = {}, zvy[4] = {};
+  if (ok && act) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      qs_z_of(A, gs_slot(ring, k, own, dt), z0 - 2 + k, x, y, qez[k], qvx[k], qvy[k]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      zvz[k] = ring.halo(k, ES_VZ)[own];
+      zvx[k] = ring.halo(k + 1, ES_VX)[own];
+      zvy[k] = ring.halo(k + 1, ES_VY)[own];
+    }
+  }
+  if (__syncthreads_or(!ok)) {
+    ring_abort(ring, 0, min(nj, R), R, tid, status);
+    return;
+  }
+  // slots 0 and 1 (planes z0-2, z0-1) are free after the queue fill
+  if (tid == 0)
+    for (int j = R; j < R + 2 && j < nj; ++j) {
+      fence_proxy_async_smem();
+      ring.issue(maps, j, y0, x0, z0 - 2 + j, z0 - 2 + j);
+    }
+
+  for (int q = 0; q < nq; ++q) {
+    const int z = z0 + q, jc = q + 2;
+    const int i = act ? cell32(g, z, x, y) : 0;
+    float av0 = 0.f, av1 = 0.f, av2 = 0.f, gi0 = 0.f, gi1 = 0.f;
+    if (act) {  // read-modify-write operands, before the wait
+      av0 = A.a.vz[i]; av1 = A.a.vx[i]; av2 = A.a.vy[i];
+      if (A.g0) { gi0 = A.g0[i]; gi1 = A.g1[i]; }
+    }
+    const bool got = ring.wait(q + 4);
+    GS G{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (got) {
+      qez[4] = qvx[4] = qvy[4] = 0.f;
+      if (act) qs_z_of(A, gs_slot(ring, q + 4, own, dt), z + 2, x, y, qez[4], qvx[4], qvy[4]);
+      zvz[3] = ring.halo(q + 3, ES_VZ)[own];
+      zvx[3] = ring.halo(q + 4, ES_VX)[own];
+      zvy[3] = ring.halo(q + 4, ES_VY)[own];
+      float ox[3] = {0.f, 0.f, 0.f}, oy[3] = {0.f, 0.f, 0.f};
+      if (act) {  // qs_own
+        G = gs_slot(ring, jc, own, dt);
+        qs_x_of(A, G, z, x, y, ox[0], ox[1], ox[2]);
+        qs_y_of(A, G, z, x, y, oy[0], oy[1], oy[2]);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { sqx[k][ty + 2][tx] = ox[k]; sqy[k][ty][tx + 2] = oy[k]; }
+      if (ty < 4) {
+        float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+        if (yin) qs_x_of(A, gs_slot(ring, jc, hro, dt), z, hxn, y, h0, h1, h2);
+        sqx[0][hr][tx] = h0; sqx[1][hr][tx] = h1; sqx[2][hr][tx] = h2;
+      }
+      if (tx < 4) {
+        float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+        if (xin) qs_y_of(A, gs_slot(ring, jc, hco, dt), z, x, hyn, h0, h1, h2);
+        sqy[0][ty][hc] = h0; sqy[1][ty][hc] = h1; sqy[2][ty][hc] = h2;
+      }
+    }
+    __syncthreads();
+    if (got && act) {
+      const float(*QX)[TX + 4][32] = sqx;
+      const float(*QY)[TX][36] = sqy;
+      // ---- adjoint velocities
+      const float dvz = -dplus(qez[1], qez[2], qez[3], qez[4]) * idz -
+                        dminus(QX[1][ty][tx], QX[1][ty + 1][tx], QX[1][ty + 2][tx], QX[1][ty + 3][tx]) * idx -
+                        dminus(QY[1][ty][tx], QY[1][ty][tx + 1], QY[1][ty][tx + 2], QY[1][ty][tx + 3]) * idy;
+      const float dvx = -dplus(QX[0][ty + 1][tx], QX[0][ty + 2][tx], QX[0][ty + 3][tx], QX[0][ty + 4][tx]) * idx -
+                        dminus(qvx[0], qvx[1], qvx[2], qvx[3]) * idz -
+                        dminus(QY[2][ty][tx], QY[2][ty][tx + 1], QY[2][ty][tx + 2], QY[2][ty][tx + 3]) * idy;
+      const float dvy = -dplus(QY[0][ty][tx + 1], QY[0][ty][tx + 2], QY[0][ty][tx + 3], QY[0][ty][tx + 4]) * idy -
+                        dminus(QX[2][ty][tx], QX[2][ty + 1][tx], QX[2][ty + 2][tx], QX[2][ty + 3][tx]) * idx -
+                        dminus(qvy[0], qvy[1], qvy[2], qvy[3]) * idz;
+
+      // ---- images from the forward velocities of the same step; box row r
+      // is x = x0 - 2 + r, box column c is y = y0 - 4 + c
+      const BoxView fz{ring.halo(jc, ES_VZ) + own}, fx{ring.halo(jc, ES_VX) + own},
+          fy{ring.halo(jc, ES_VY) + own};
+      float ezz = dminus(zvz[0], zvz[1], zvz[2], zvz[3]) * idz;
+      float exx = dminus(fx.x(-2), fx.x(-1), fx.c(), fx.x(1)) * idx;
+      float eyy = dminus(fy.y(-2), fy.y(-1), fy.c(), fy.y(1)) * idy;
+      float dvx_dz = dplus(zvx[0], zvx[1], zvx[2], zvx[3]) * idz;
+      float dvy_dz = dplus(zvy[0], zvy[1], zvy[2], zvy[3]) * idz;
+      float dvx_dy = dplus(fx.y(-1), fx.c(), fx.y(1), fx.y(2)) * idy;
+      float dvz_dx = dplus(fz.x(-1), fz.c(), fz.x(1), fz.x(2)) * idx;
+      float dvz_dy = dplus(fz.y(-1), fz.c(), fz.y(1), fz.y(2)) * idy;
+      float dvy_dx = dplus(fy.x(-1), fy.c(), fy.x(1), fy.x(2)) * idx;
+      if (slab_s(z, nz, np)) {
+        const float *c = g.cz;
+        const float Kz = c[CK * nz + z], az = c[CA * nz + z], bz = c[CB * nz + z];
+        const float Kzh = c[CKH * nz + z], azh = c[CAH * nz + z], bzh = c[CBH * nz + z];
+        const int k = psi32_z(g, z, x, y);
+        const float *p = A.ps.z;
+        ezz = ezz * Kz + (bz * p[PSI_VA * (int)g.slab_z + k] + az * ezz);
+        dvx_dz = dvx_dz * Kzh + (bzh * p[PSI_VB1 * (int)g.slab_z + k] + azh * dvx_dz);
+        dvy_dz = dvy_dz * Kzh + (bzh * p[PSI_VB2 * (int)g.slab_z + k] + azh * dvy_dz);
+        A.lout.z[PSI_VA * (int)g.slab_z + k] = bz * (A.lin.z[PSI_VA * (int)g.slab_z + k] + G.ez);
+        A.lout.z[PSI_VB1 * (int)g.slab_z + k] = bzh * (A.lin.z[PSI_VB1 * (int)g.slab_z + k] + G.xz);
+        A.lout.z[PSI_VB2 * (int)g.slab_z + k] = bzh * (A.lin.z[PSI_VB2 * (int)g.slab_z + k] + G.yz);
+      }
+      if (xs) {
+        const float *c = g.cx;
+        const float Kx = c[CK * nx + x], ax = c[CA * nx + x], bx = c[CB * nx + x];
+        const float Kxh = c[CKH * nx + x], axh = c[CAH * nx + x], bxh = c[CBH * nx + x];
+        const int k = psi32_x(g, z, x, y);
+        const float *p = A.ps.x;
+        exx = exx * Kx + (bx * p[PSI_VA * (int)g.slab_x + k] + ax * exx);
+        dvz_dx = dvz_dx * Kxh + (bxh * p[PSI_VB1 * (int)g.slab_x + k] + axh * dvz_dx);
+        dvy_dx = dvy_dx * Kxh + (bxh * p[PSI_VB2 * (int)g.slab_x + k] + axh * dvy_dx);
+        A.lout.x[PSI_VA * (int)g.slab_x + k] = bx * (A.lin.x[PSI_VA * (int)g.slab_x + k] + G.ex);
+        A.lout.x[PSI_VB1 * (int)g.slab_x + k] = bxh * (A.lin.x[PSI_VB1 * (int)g.slab_x + k] + G.xz);
+        A.lout.x[PSI_VB2 * (int)g.slab_x + k] = bxh * (A.lin.x[PSI_VB2 * (int)g.slab_x + k] + G.xy);
+      }
+      if (ys) {
+        const float *c = g.cy;
+        const float Ky = c[CK * ny + y], ay = c[CA * ny + y], by = c[CB * ny + y];
+        const float Kyh = c[CKH * ny + y], ayh = c[CAH * ny + y], byh = c[CBH * ny + y];
+        const int k = psi32_y(g, z, x, y);
+        const float *p = A.ps.y;
+        eyy = eyy * Ky + (by * p[PSI_VA * (int)g.slab_y + k] + ay * eyy);
+        dvz_dy = dvz_dy * Kyh + (byh * p[PSI_VB1 * (int)g.slab_y + k] + ayh * dvz_dy);
+        dvx_dy = dvx_dy * Kyh + (byh * p[PSI_VB2 * (int)g.slab_y + k] + ayh * dvx_dy);
+        A.lout.y[PSI_VA * (int)g.slab_y + k] = by * (A.lin.y[PSI_VA * (int)g.slab_y + k] + G.ey);
+        A.lout.y[PSI_VB1 * (int)g.slab_y + k] = byh * (A.lin.y[PSI_VB1 * (int)g.slab_y + k] + G.yz);
+        A.lout.y[PSI_VB2 * (int)g.slab_y + k] = byh * (A.lin.y[PSI_VB2 * (int)g.slab_y + k] + G.xy);
+      }
+      if (A.g0) {
+        const float azz = ring.halo(jc, ES_ZZ)[own], axx = ring.halo(jc, ES_XX)[own],
+                    ayy = ring.halo(jc, ES_YY)[own];
+        const float axz = ring.halo(jc, ES_XZ)[own], axy = ring.halo(jc, ES_XY)[own],
+                    ayz = ring.halo(jc, ES_YZ)[own];
+        A.g0[i] = gi0 + (azz + axx + ayy) * (ezz + exx + eyy) * dt;
+        A.g1[i] = gi1 + (2.0f * (azz * ezz + axx * exx + ayy * eyy) + axz * (dvx_dz + dvz_dx) +
+                         axy * (dvx_dy + dvy_dx) + ayz * (dvy_dz + dvz_dy)) * dt;
+      }
+      A.a.vz[i] = av0 + dvz;
+      A.a.vx[i] = av1 + dvx;
+      A.a.vy[i] = av2 + dvy;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { qez[k] = qez[k + 1]; qvx[k] = qvx[k + 1]; qvy[k] = qvy[k + 1]; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { zvz[k] = zvz[k + 1]; zvx[k] = zvx[k + 1]; zvy[k] = zvy[k + 1]; }
+    if (__syncthreads_or(!got)) {
+      ring_abort(ring, q + 4, min(nj, q + 2 + R), R, tid, status);
+      return;
+    }
+    const int jn = jc + R;  // the slot of plane z is free: refill it
+    if (tid == 0 && jn < nj) {
+      fence_proxy_async_smem();
+      ring.issue(maps, jn, y0, x0, z0 - 2 + jn, z0 - 2 + jn);
+    }
+  }
+}
+
+// G of the velocity stage from slot values (gv_at).
+template <class Ring>
+__device__ __forceinline__ void gv_slot(const Ring &ring, int j, int o, float dt, float &gz,
+                                        float &gx, float &gy) {
+  const float s = ring.halo(j, EV_B)[o] * dt;
+  gz = ring.halo(j, EV_VZ)[o] * s;
+  gx = ring.halo(j, EV_VX)[o] * s;
+  gy = ring.halo(j, EV_VY)[o] * s;
+}
+
+// z-, x- and y-axis terms of the velocity stage from G (qv_z, qv_x, qv_y).
+__device__ __forceinline__ void qv_z_of(const ExactArgs &A, float gz, float gx, float gy, int zn,
+                                        int x, int y, float &qzz, float &qxz, float &qyz) {
+  const Geo &g = A.g;
+  if (zn < 2 || zn > g.nz - 3) { qzz = qxz = qyz = 0.f; return; }
+  if (slab_s(zn, g.nz, g.np)) {
+    const int k = psi32_z(g, zn, x, y);
+    const float *c = g.cz;
+    const int nz = g.nz;
+    qzz = qpml(gz, true, A.lin.z[PSI_SAA * (int)g.slab_z + k], c[CKH * nz + zn], c[CAH * nz + zn]);
+    qxz = qpml(gx, true, A.lin.z[PSI_SAB1 * (int)g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+    qyz = qpml(gy, true, A.lin.z[PSI_SAB2 * (int)g.slab_z + k], c[CK * nz + zn], c[CA * nz + zn]);
+  } else {
+    qzz = gz; qxz = gx; qyz = gy;
+  }
+}
+
+__device__ __forceinline__ void qv_x_of(const ExactArgs &A, float gz, float gx, float gy, int z,
+                                        int xn, int y, float &qxz, float &qxx, float &qxy) {
+  const Geo &g = A.g;
+  if (xn < 2 || xn > g.nx - 3) { qxz = qxx = qxy = 0.f; return; }
+  if (slab_v(xn, g.nx, g.np)) {
+    const int k = psi32_x(g, z, xn, y);
+    const float *c = g.cx;
+    const int nx = g.nx;
+    qxz = qpml(gz, true, A.lin.x[PSI_SAB1 * (int)g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+    qxx = qpml(gx, true, A.lin.x[PSI_SAA * (int)g.slab_x + k], c[CKH * nx + xn], c[CAH * nx + xn]);
+    qxy = qpml(gy, true, A.lin.x[PSI_SAB2 * (int)g.slab_x + k], c[CK * nx + xn], c[CA * nx + xn]);
+  } else {
+    qxz = gz; qxx = gx; qxy = gy;
+  }
+}
+
+__device__ __forceinline__ void qv_y_of(const ExactArgs &A, float gz, float gx, float gy, int z,
+                                        int x, int yn, float &qyz, float &qxy, float &qyy) {
+  const Geo &g = A.g;
+  if (yn < 2 || yn > g.ny - 3) { qyz = qxy = qyy = 0.f; return; }
+  if (slab_v(yn, g.ny, g.np)) {
+    const int k = psi32_y(g, z, x, yn);
+    const float *c = g.cy;
+    const int ny = g.ny;
+    qyz = qpml(gz, true, A.lin.y[PSI_SAB1 * (int)g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qxy = qpml(gx, true, A.lin.y[PSI_SAB2 * (int)g.slab_y + k], c[CK * ny + yn], c[CA * ny + yn]);
+    qyy = qpml(gy, true, A.lin.y[PSI_SAA * (int)g.slab_y + k], c[CKH * ny + yn], c[CAH * ny + yn]);
+  } else {
+    qyz = gz; qxy = gx; qyy = gy;
+  }
+}
+
+template <int TX, int R, int MINB>
+__global__ void __launch_bounds__(32 * TX, MINB)
+k_adj_velocity_tma(const __grid_constant__ Maps<EV_N> maps, ExactArgs A, int zchunk, int *status) {
+  using Ring = PlaneRing<EV_N, 0, 0, TX, R>;
+  __shared__ float sqx[3][TX + 4][32];
+  __shared__ float sqy[3][TX][36];
+  extern __shared__ __align__(128) unsigned char smem[];
+  Ring ring;
+  ring.bind(smem);
+  const Geo &g = A.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int y0 = blockIdx.x * 32, x0 = blockIdx.y * TX;
+  const int y = y0 + tx, x = x0 + ty;
+  const int z0 = max((int)blockIdx.z * zchunk, 2);
+  const int z1 = min((int)blockIdx.z * zchunk + zchunk, g.nz - 2);
+  if (z0 >= z1) return;
+  const int nq = z1 - z0, nj = nq + 4;
+  if (tid == 0) ring.init();
+  __syncthreads();
+  if (tid == 0)
+    for (int j = 0; j < nj && j < R; ++j) ring.issue(maps, j, y0, x0, z0 - 2 + j, z0 - 2 + j);
+
+  const int np = g.np, nz = g.nz, nx = g.nx, ny = g.ny;
+  const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
+  const bool xin = x >= 2 && x <= nx - 3, yin = y >= 2 && y <= ny - 3;
+  const bool act = xin && yin;
+  const bool xs = slab_v(x, nx, np), ys = slab_v(y, ny, np);
+  const int hr = ty < 2 ? ty : TX + ty;
+  const int hxn = x0 - 2 + hr;
+  const int hc = tx < 2 ? tx : 32 + tx;
+  const int hyn = y0 - 2 + hc;
+  const int own = (ty + TMA_HX) * TMA_BOXY + tx + TMA_HY;
+  const int hro = hr * TMA_BOXY + tx + TMA_HY;
+  const int hco = (ty + TMA_HX) * TMA_BOXY + hc + 2;
+
+  bool ok = true;
+  for (int j = 0; j < 4; ++j) ok = ring.wait(j) && ok;
+  // queues: Q_z of planes z-2 .. z+2; forward szz at z-1 .. z+2, sxz and
+  // syz at z-2 .. z+1
+  float qzz[5] = {}, qxz[5] = {}, qyz[5] = {};
+  float zszz[4] = {}, zsxz[4] = {}, zsyz[4] = {};
+  if (ok && act) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float gz, gx, gy;
+      gv_slot(ring, k, own, dt, gz, gx, gy);
+      qv_z_of(A, gz, gx, gy, z0 - 2 + k, x, y, qzz[k], qxz[k], qyz[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      zszz[k] = ring.halo(k + 1, EV_SZZ)[own];
+      zsxz[k] = ring.halo(k, EV_SXZ)[own];
+      zsyz[k] = ring.halo(k, EV_SYZ)[own];
+    }
+  }
+  if (__syncthreads_or(!ok)) {
+    ring_abort(ring, 0, min(nj, R), R, tid, status);
+    return;
+  }
+  if (tid == 0)
+    for (int j = R; j < R + 2 && j < nj; ++j) {
+      fence_proxy_async_smem();
+      ring.issue(maps, j, y0, x0, z0 - 2 + j, z0 - 2 + j);
+    }
+
+  for (int q = 0; q < nq; ++q) {
+    const int z = z0 + q, jc = q + 2;
+    const int i = act ? cell32(g, z, x, y) : 0;
+    float as0 = 0.f, as1 = 0.f, as2 = 0.f, as3 = 0.f, as4 = 0.f, as5 = 0.f, gi0 = 0.f;
+    if (act) {  // read-modify-write operands, before the wait
+      as0 = A.a.szz[i]; as1 = A.a.sxx[i]; as2 = A.a.syy[i];
+      as3 = A.a.sxz[i]; as4 = A.a.syz[i]; as5 = A.a.sxy[i];
+      if (A.g0) gi0 = A.g0[i];
+    }
+    const bool got = ring.wait(q + 4);
+    float gz = 0.f, gx = 0.f, gy = 0.f;
+    if (got) {
+      qzz[4] = qxz[4] = qyz[4] = 0.f;
+      if (act) {
+        float hz, hx, hy;
+        gv_slot(ring, q + 4, own, dt, hz, hx, hy);
+        qv_z_of(A, hz, hx, hy, z + 2, x, y, qzz[4], qxz[4], qyz[4]);
+      }
+      zszz[3] = ring.halo(q + 4, EV_SZZ)[own];
+      zsxz[3] = ring.halo(q + 3, EV_SXZ)[own];
+      zsyz[3] = ring.halo(q + 3, EV_SYZ)[own];
+      float ox[3] = {0.f, 0.f, 0.f}, oy[3] = {0.f, 0.f, 0.f};
+      if (act) {  // qv_own
+        gv_slot(ring, jc, own, dt, gz, gx, gy);
+        qv_x_of(A, gz, gx, gy, z, x, y, ox[0], ox[1], ox[2]);
+        qv_y_of(A, gz, gx, gy, z, x, y, oy[0], oy[1], oy[2]);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { sqx[k][ty + 2][tx] = ox[k]; sqy[k][ty][tx + 2] = oy[k]; }
+      if (ty < 4) {
+        float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+        if (yin) {
+          float hz, hx, hy;
+          gv_slot(ring, jc, hro, dt, hz, hx, hy);
+          qv_x_of(A, hz, hx, hy, z, hxn, y, h0, h1, h2);
+        }
+        sqx[0][hr][tx] = h0; sqx[1][hr][tx] = h1; sqx[2][hr][tx] = h2;
+      }
+      if (tx < 4) {
+        float h0 = 0.f, h1 = 0.f, h2 = 0.f;
+        if (xin) {
+          float hz, hx, hy;
+          gv_slot(ring, jc, hco, dt, hz, hx, hy);
+          qv_y_of(A, hz, hx, hy, z, x, hyn, h0, h1, h2);
+        }
+        sqy[0][ty][hc] = h0; sqy[1][ty][hc] = h1; sqy[2][ty][hc] = h2;
+      }
+    }
+    __syncthreads();
+    if (got && act) {
+      const float(*QX)[TX + 4][32] = sqx;
+      const float(*QY)[TX][36] = sqy;
+      // ---- adjoint stresses (x: 0 vz<-sxz, 1 vx<-sxx, 2 vy<-sxy;
+      //                        y: 0 vz<-syz, 1 vx<-sxy, 2 vy<-syy)
+      const float dszz = -dminus(qzz[0], qzz[1], qzz[2], qzz[3]) * idz;
+      const float dsxx = -dminus(QX[1][ty][tx], QX[1][ty + 1][tx], QX[1][ty + 2][tx], QX[1][ty + 3][tx]) * idx;
+      const float dsyy = -dminus(QY[2][ty][tx], QY[2][ty][tx + 1], QY[2][ty][tx + 2], QY[2][ty][tx + 3]) * idy;
+      const float dsxz = -dplus(QX[0][ty + 1][tx], QX[0][ty + 2][tx], QX[0][ty + 3][tx], QX[0][ty + 4][tx]) * idx -
+                         dplus(qxz[1], qxz[2], qxz[3], qxz[4]) * idz;
+      const float dsyz = -dplus(QY[0][ty][tx + 1], QY[0][ty][tx + 2], QY[0][ty][tx + 3], QY[0][ty][tx + 4]) * idy -
+                         dplus(qyz[1], qyz[2], qyz[3], qyz[4]) * idz;
+      const float dsxy = -dplus(QY[1][ty][tx + 1], QY[1][ty][tx + 2], QY[1][ty][tx + 3], QY[1][ty][tx + 4]) * idy +
+                         dq_t(QX[2][ty + 2][tx], QX[2][ty + 3][tx], QX[2][ty + 4][tx]) * idx;
+
+      // ---- buoyancy image from the forward stresses of the same step
+      const BoxView fxz{ring.halo(jc, EV_SXZ) + own}, fxx{ring.halo(jc, EV_SXX) + own},
+          fxy{ring.halo(jc, EV_SXY) + own}, fyz{ring.halo(jc, EV_SYZ) + own},
+          fyy{ring.halo(jc, EV_SYY) + own};
+      float dszz_dz = dplus(zszz[0], zszz[1], zszz[2], zszz[3]) * idz;
+      float dsxz_dx = dminus(fxz.x(-2), fxz.x(-1), fxz.c(), fxz.x(1)) * idx;
+      float dsyz_dy = dminus(fyz.y(-2), fyz.y(-1), fyz.c(), fyz.y(1)) * idy;
+      float dsxz_dz = dminus(zsxz[0], zsxz[1], zsxz[2], zsxz[3]) * idz;
+      float dsxx_dx = dplus(fxx.x(-1), fxx.c(), fxx.x(1), fxx.x(2)) * idx;
+      float dsxy_dy = dminus(fxy.y(-2), fxy.y(-1), fxy.c(), fxy.y(1)) * idy;
+      float dsyz_dz = dminus(zsyz[0], zsyz[1], zsyz[2], zsyz[3]) * idz;
+      const float sxy0 = fxy.c(), sxym1 = fxy.x(-1), sxym2 = fxy.x(-2);
+      float dsxy_dx = (EFWI_C1 * (sxy0 - sxym1) - EFWI_C2 * (sxym1 - sxym2)) * idx;
+      float dsyy_dy = dplus(fyy.y(-1), fyy.c(), fyy.y(1), fyy.y(2)) * idy;
+      if (slab_s(z, nz, np)) {
+        const float *c = g.cz;
+        const float Kz = c[CK * nz + z], bz = c[CB * nz + z], Kzh = c[CKH * nz + z], bzh = c[CBH * nz + z];
+        const int k = psi32_z(g, z, x, y);
+        const float *p = A.ps.z;
+        dszz_dz = dszz_dz * Kzh + p[PSI_SAA * (int)g.slab_z + k];
+        dsxz_dz = dsxz_dz * Kz + p[PSI_SAB1 * (int)g.slab_z + k];
+        dsyz_dz = dsyz_dz * Kz + p[PSI_SAB2 * (int)g.slab_z + k];
+        A.lout.z[PSI_SAA * (int)g.slab_z + k] = bzh * (A.lin.z[PSI_SAA * (int)g.slab_z + k] + gz);
+        A.lout.z[PSI_SAB1 * (int)g.slab_z + k] = bz * (A.lin.z[PSI_SAB1 * (int)g.slab_z + k] + gx);
+        A.lout.z[PSI_SAB2 * (int)g.slab_z + k] = bz * (A.lin.z[PSI_SAB2 * (int)g.slab_z + k] + gy);
+      }
+      if (xs) {
+        const float *c = g.cx;
+        const float Kx = c[CK * nx + x], bx = c[CB * nx + x], Kxh = c[CKH * nx + x], bxh = c[CBH * nx + x];
+        const int k = psi32_x(g, z, x, y);
+        const float *p = A.ps.x;
+        dsxz_dx = dsxz_dx * Kx + p[PSI_SAB1 * (int)g.slab_x + k];
+        dsxx_dx = dsxx_dx * Kxh + p[PSI_SAA * (int)g.slab_x + k];
+        dsxy_dx = dsxy_dx * Kx + p[PSI_SAB2 * (int)g.slab_x + k];
+        A.lout.x[PSI_SAB1 * (int)g.slab_x + k] = bx * (A.lin.x[PSI_SAB1 * (int)g.slab_x + k] + gz);
+        A.lout.x[PSI_SAA * (int)g.slab_x + k] = bxh * (A.lin.x[PSI_SAA * (int)g.slab_x + k] + gx);
+        A.lout.x[PSI_SAB2 * (int)g.slab_x + k] = bx * (A.lin.x[PSI_SAB2 * (int)g.slab_x + k] + gy);
+      }
+      if (ys) {
+        const float *c = g.cy;
+        const float Ky = c[CK * ny + y], by = c[CB * ny + y], Kyh = c[CKH * ny + y], byh = c[CBH * ny + y];
+        const int k = psi32_y(g, z, x, y);
+        const float *p = A.ps.y;
+        dsyz_dy = dsyz_dy * Ky + p[PSI_SAB1 * (int)g.slab_y + k];
+        dsxy_dy = dsxy_dy * Ky + p[PSI_SAB2 * (int)g.slab_y + k];
+        dsyy_dy = dsyy_dy * Kyh + p[PSI_SAA * (int)g.slab_y + k];
+        A.lout.y[PSI_SAB1 * (int)g.slab_y + k] = by * (A.lin.y[PSI_SAB1 * (int)g.slab_y + k] + gz);
+        A.lout.y[PSI_SAB2 * (int)g.slab_y + k] = by * (A.lin.y[PSI_SAB2 * (int)g.slab_y + k] + gx);
+        A.lout.y[PSI_SAA * (int)g.slab_y + k] = byh * (A.lin.y[PSI_SAA * (int)g.slab_y + k] + gy);
+      }
+      if (A.g0) {
+        const float avz = ring.halo(jc, EV_VZ)[own], avx = ring.halo(jc, EV_VX)[own],
+                    avy = ring.halo(jc, EV_VY)[own];
+        A.g0[i] = gi0 + (avz * (dszz_dz + dsxz_dx + dsyz_dy) + avx * (dsxz_dz + dsxx_dx + dsxy_dy) +
+                         avy * (dsyz_dz + dsxy_dx + dsyy_dy)) * dt;
+      }
+      A.a.szz[i] = as0 + dszz;
+      A.a.sxx[i] = as1 + dsxx;
+      A.a.syy[i] = as2 + dsyy;
+      A.a.sxz[i] = as3 + dsxz;
+      A.a.syz[i] = as4 + dsyz;
+      A.a.sxy[i] = as5 + dsxy;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { qzz[k] = qzz[k + 1]; qxz[k] = qxz[k + 1]; qyz[k] = qyz[k + 1]; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { zszz[k] = zszz[k + 1]; zsxz[k] = zsxz[k + 1]; zsyz[k] = zsyz[k + 1]; }
+    if (__syncthreads_or(!got)) {
+      ring_abort(ring, q + 4, min(nj, q + 2 + R), R, tid, status);
+      return;
+    }
+    const int jn = jc + R;
+    if (tid == 0 && jn < nj) {
+      fence_proxy_async_smem();
+      ring.issue(maps, jn, y0, x0, z0 - 2 + jn, z0 - 2 + jn);
+    }
+  }
+}
+
 }  // namespace
 
 void launch_adj_stress_exact(int bx, dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk,
@@ -644,6 +1189,37 @@ void launch_adj_velocity_exact(int bx, dim3 grid, cudaStream_t st, const ExactAr
     k_adj_velocity_exact<8><<<grid, dim3(32, 8), 0, st>>>(A, zchunk, nzc);
   else
     k_adj_velocity_exact<4><<<grid, dim3(32, 4), 0, st>>>(A, zchunk, nzc);
+}
+
+// Bulk-copy staged exact kernels: tile 32 x TX, ring of R planes.
+template <int TX, int R, int MINB>
+static void adj_stress_tma_launch(dim3 grid, cudaStream_t st, const Maps<11> &maps,
+                                  const ExactArgs &A, int zchunk, int *status) {
+  constexpr int B = PlaneRing<ES_N, 0, 0, TX, R>::BYTES;
+  static std::atomic<unsigned long long> smem_set{0};
+  set_smem_once(k_adj_stress_tma<TX, R, MINB>, B, smem_set);
+  k_adj_stress_tma<TX, R, MINB><<<grid, dim3(32, TX), B, st>>>(maps, A, zchunk, status);
+}
+
+template <int TX, int R, int MINB>
+static void adj_velocity_tma_launch(dim3 grid, cudaStream_t st, const Maps<10> &maps,
+                                    const ExactArgs &A, int zchunk, int *status) {
+  constexpr int B = PlaneRing<EV_N, 0, 0, TX, R>::BYTES;
+  static std::atomic<unsigned long long> smem_set{0};
+  set_smem_once(k_adj_velocity_tma<TX, R, MINB>, B, smem_set);
+  k_adj_velocity_tma<TX, R, MINB><<<grid, dim3(32, TX), B, st>>>(maps, A, zchunk, status);
+}
+
+void launch_adj_stress_tma(int bx, dim3 grid, cudaStream_t st, const Maps<11> &maps,
+                           const ExactArgs &A, int zchunk, int *status) {
+  if (bx == 8) adj_stress_tma_launch<8, 5, 2>(grid, st, maps, A, zchunk, status);
+  else adj_stress_tma_launch<4, 5, 3>(grid, st, maps, A, zchunk, status);
+}
+
+void launch_adj_velocity_tma(int bx, dim3 grid, cudaStream_t st, const Maps<10> &maps,
+                             const ExactArgs &A, int zchunk, int *status) {
+  if (bx == 8) adj_velocity_tma_launch<8, 5, 2>(grid, st, maps, A, zchunk, status);
+  else adj_velocity_tma_launch<4, 5, 3>(grid, st, maps, A, zchunk, status);
 }
 
 // dJ/dstf of step k: the source adds 1500^2 * dt * w^2(k) * stf(k) to szz,

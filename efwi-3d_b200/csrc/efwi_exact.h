@@ -1,6 +1,7 @@
 // Exact discrete adjoint kernels (efwi_exact.cu).
 #pragma once
 #include "efwi_common.cuh"
+#include "efwi_tma.cuh"
 
 namespace efwi {
 
@@ -21,6 +22,14 @@ void launch_adj_stress_exact(int bx, dim3 grid, cudaStream_t st, const ExactArgs
                              int nzc);
 void launch_adj_velocity_exact(int bx, dim3 grid, cudaStream_t st, const ExactArgs &A, int zchunk,
                                int nzc);
+// The same with every plane's operands staged by bulk tensor copies (bitwise
+// the same results).  Stress stage maps (halo boxes): adjoint szz sxx syy sxz
+// sxy syz, lambda, mu, forward vz vx vy.  Velocity stage maps: adjoint vz vx
+// vy, buoyancy, forward sxz sxx sxy syz syy szz.
+void launch_adj_stress_tma(int bx, dim3 grid, cudaStream_t st, const Maps<11> &maps,
+                           const ExactArgs &A, int zchunk, int *status);
+void launch_adj_velocity_tma(int bx, dim3 grid, cudaStream_t st, const Maps<10> &maps,
+                             const ExactArgs &A, int zchunk, int *status);
 
 __global__ void k_buoy_to_rho(const float *gB, const float *buoy, float *grho, int nz, int nx,
                               int ny, int py);

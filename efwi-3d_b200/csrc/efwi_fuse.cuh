@@ -1,20 +1,15 @@
 // Receiver gather, adjoint-source injection and boundary-shell save/restore
-// fused into the stencil kernels' epilogues (the reference runs them as
-// separate kernels every step: recording and res_injection,
-// utilities.cu:481-507; from_bnd / to_bnd, utilities.cu:323-420 with
-// Boundary.cu:59-138).
+// in the stencil kernels' epilogues (the reference runs them as separate
+// kernels every step: recording and res_injection, utilities.cu:481-507;
+// from_bnd / to_bnd, utilities.cu:323-420 with Boundary.cu:59-138).
 //
 // Shell: the points of the reference's 5-cell boundary shell inside
 // [2, n-3]^3 are stored per step as [9][npts] in (z, x, y) order.  A row
-// (z, x) of the grid holds either no shell point, a full run of points
-// y in [ya0, yb1], or two runs [ya0, ya1] and [yb0, yb1]; rows[z * nx + x]
-// gives the index of the row's first point (bit 30 set for a split row) or
-// -1.  So a thread finds its cell's shell index in O(1) from one load that
-// is uniform over its warp.
-//
-// Receivers: for the planes that hold receiver cells of a launch's shots,
-// plane[s * nz + z] names a map [nx][py] of unique receiver cell numbers
-// (RecArgs::ucell order, -1 elsewhere); other planes read -1.
+// (z, x) of the grid holds no shell point, one run of points y in
+// [ya0, yb1], or two runs [ya0, ya1] and [yb0, yb1] (ShellMap), so a thread
+// finds its cell's shell index in O(1) from one row entry that is uniform
+// over its warp.  Receivers: a per-plane map of unique receiver cells
+// (RecArgs::plane, RecArgs::map).
 #pragma once
 #include "efwi_common.cuh"
 #include "efwi_kernels.h"
@@ -23,21 +18,8 @@ namespace efwi {
 
 constexpr int SHELL_SPLIT = 1 << 30;
 
-struct ShellMap {
-  const int *rows;  // [nz][nx] (nullptr: no shell work)
-  float *store;     // [9][npts] of the current step
-  int npts;
-  int ya0, ya1, yb0, yb1;
-};
-
-struct RecMap {
-  const int *plane;  // [nshot][nz] (nullptr: no receiver work)
-  const int *map;    // [nmaps][nx][py]
-  int nxpy;
-};
-
-// Shell point index of cell (z, x, y) from its row entry, or -1.
-__device__ __forceinline__ int shell_index(const ShellMap &s, int row, int y) {
+// Shell point index of a cell at y whose row entry is `row`, or -1.
+__host__ __device__ __forceinline__ int shell_index(const ShellMap &s, int row, int y) {
   if (row < 0) return -1;
   const int base = row & ~SHELL_SPLIT;
   if (!(row & SHELL_SPLIT)) return (y >= s.ya0 && y <= s.yb1) ? base + y - s.ya0 : -1;
@@ -47,12 +29,11 @@ __device__ __forceinline__ int shell_index(const ShellMap &s, int row, int y) {
 }
 
 // Unique receiver cell at (shot, z, x, y), or -1.
-__device__ __forceinline__ int receiver_at(const RecMap &m, int nz, int py, int shot, int z, int x,
-                                           int y) {
-  if (!m.plane) return -1;
-  const int mp = m.plane[shot * nz + z];
+__device__ __forceinline__ int receiver_at(const RecArgs &r, int nz, int py, int shot, int z,
+                                           int x, int y) {
+  const int mp = r.plane[shot * nz + z];
   if (mp < 0) return -1;
-  return m.map[(long long)mp * m.nxpy + x * py + y];
+  return r.map[(long long)mp * r.nxpy + x * py + y];
 }
 
 // recording (utilities.cu:481-495) of unique receiver cell u at sample it.
@@ -83,19 +64,5 @@ __device__ __forceinline__ void inject_cell(const RecArgs &rec, const float *res
     vz += t[2 * nr + r];
   }
 }
-
-}  // namespace efwi
-
-namespace efwi {
-
-// Receiver work of one launch: the maps, the grouping, the time-major trace
-// array (recorded into by the forward velocity kernel, read as the
-// adjoint source by the reverse velocity kernel) and the sample index.
-struct RecFuse {
-  RecMap m;
-  RecArgs a;
-  float *tm;
-  int it;
-};
 
 }  // namespace efwi

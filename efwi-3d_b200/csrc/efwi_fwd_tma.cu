@@ -8,7 +8,12 @@
 // Results are stored straight from registers (one 128-byte row per warp).
 // Restated reference kernels: stress.cu:36-97, add_source
 // (utilities.cu:442-479), velocity.cu:35-96 (quirks Q1 and Q2 kept).
+//
+// Fused epilogues (efwi_fuse.cuh): K_S stores the step's starting state at
+// the boundary-shell points (gradient sweeps, from_bnd); K_V records the
+// receivers (recording).
 #include "efwi_common.cuh"
+#include "efwi_fuse.cuh"
 #include "efwi_kernels.h"
 #include "efwi_tma.cuh"
 
@@ -19,7 +24,7 @@ constexpr int FWD_RING = 4;
 template <int TX, int R, int MINB>
 __global__ void __launch_bounds__(32 * TX, MINB)
 k_stress_fwd_tma(const __grid_constant__ Maps<11> maps, Geo g, Fields f, Psi ps, int zchunk,
-                 int nzc, SrcArgs src, int *status) {
+                 int nzc, SrcArgs src, ShellMap shell, int *status) {
   using Ring = PlaneRing<3, 8, 2, TX, R>;  // vz vx vy | szz sxx syy sxz sxy syz | lam mu
   extern __shared__ __align__(128) unsigned char smem[];
   Ring ring;
@@ -87,6 +92,9 @@ k_stress_fwd_tma(const __grid_constant__ Maps<11> maps, Geo g, Fields f, Psi ps,
         prefetch_l2(vz + i + 3 * sz); prefetch_l2(vx + i + 4 * sz); prefetch_l2(vy + i + 4 * sz);
       }
     }
+    // shell row of this plane, loaded before the wait so that its latency
+    // overlaps it
+    const int srow = (shell.rows && act) ? shell.rows[z * nx + x] : -1;
     const bool got = ring.wait(q);
     if (act && got) {
       const BoxView bz{ring.halo(q, 0) + off}, bxv{ring.halo(q, 1) + off},
@@ -134,6 +142,17 @@ k_stress_fwd_tma(const __grid_constant__ Maps<11> maps, Geo g, Fields f, Psi ps,
         pyb[PSI_VB2 * g.slab_y + k] = m; dvx_dy = dvx_dy * Kyh + m;
       }
       const float l = ring.point(q, 6)[pt], u = ring.point(q, 7)[pt], l2u = l + 2.0f * u;
+      {  // from_bnd: the state at the start of the step
+        const int sk = shell_index(shell, srow, y);
+        if (sk >= 0) {
+          float *st = shell.store + sk;
+          const int n = shell.npts;
+          st[0] = ring.point(q, 0)[pt]; st[n] = ring.point(q, 3)[pt];
+          st[2 * n] = ring.point(q, 1)[pt]; st[3 * n] = ring.point(q, 2)[pt];
+          st[4 * n] = ring.point(q, 4)[pt]; st[5 * n] = ring.point(q, 5)[pt];
+          st[6 * n] = qz2; st[7 * n] = qx1; st[8 * n] = qy1;
+        }
+      }
       float nzz = ring.point(q, 0)[pt] + (l2u * ezz + l * exx + l * eyy) * dt;
       float nxx = ring.point(q, 1)[pt] + (l * ezz + l2u * exx + l * eyy) * dt;
       float nyy = ring.point(q, 2)[pt] + (l * ezz + l * exx + l2u * eyy) * dt;
@@ -167,7 +186,7 @@ k_stress_fwd_tma(const __grid_constant__ Maps<11> maps, Geo g, Fields f, Psi ps,
 template <int TX, int R, int MINB>
 __global__ void __launch_bounds__(32 * TX, MINB)
 k_velocity_fwd_tma(const __grid_constant__ Maps<9> maps, Geo g, Fields f, Psi ps, int zchunk,
-                   int nzc, int *status) {
+                   int nzc, RecFuse rec, int *status) {
   using Ring = PlaneRing<5, 4, 1, TX, R>;  // sxz syz sxx sxy syy | vz vx vy | buoy
   extern __shared__ __align__(128) unsigned char smem[];
   Ring ring;
@@ -232,6 +251,8 @@ k_velocity_fwd_tma(const __grid_constant__ Maps<9> maps, Geo g, Fields f, Psi ps
         prefetch_l2(szz + i + 4 * sz); prefetch_l2(sxz + i + 3 * sz); prefetch_l2(syz + i + 3 * sz);
       }
     }
+    // receiver map of this plane (-1: none), loaded before the wait
+    const int rmap = rec.a.plane ? rec.a.plane[shot * nz + z] : -1;
     const bool got = ring.wait(q);
     if (act && got) {
       const BoxView bxz{ring.halo(q, 0) + off}, byz{ring.halo(q, 1) + off};
@@ -283,9 +304,14 @@ k_velocity_fwd_tma(const __grid_constant__ Maps<9> maps, Geo g, Fields f, Psi ps
         m = byh * pyb[PSI_SAA * g.slab_y + k] + ayh * dsyy_dy;
         pyb[PSI_SAA * g.slab_y + k] = m; dsyy_dy = dsyy_dy * Kyh + m;
       }
-      vz[i] = ring.point(q, 0)[pt] + (dszz_dz + dsxz_dx + dsyz_dy) * b * dt;
-      vx[i] = ring.point(q, 1)[pt] + (dsxz_dz + dsxx_dx + dsxy_dy) * b * dt;
-      vy[i] = ring.point(q, 2)[pt] + (dsyz_dz + dsxy_dx + dsyy_dy) * b * dt;
+      const float nvz = ring.point(q, 0)[pt] + (dszz_dz + dsxz_dx + dsyz_dy) * b * dt;
+      const float nvx = ring.point(q, 1)[pt] + (dsxz_dz + dsxx_dx + dsxy_dy) * b * dt;
+      const float nvy = ring.point(q, 2)[pt] + (dsyz_dz + dsxy_dx + dsyy_dy) * b * dt;
+      vz[i] = nvz; vx[i] = nvx; vy[i] = nvy;
+      if (rmap >= 0) {
+        const int u = rec.a.map[(long long)rmap * rec.a.nxpy + x * g.sx + y];
+        if (u >= 0) record_cell(rec.a, rec.tm, rec.it, u, nvz, nvx, nvy);
+      }
     }
     qa0 = qa1; qa1 = qa2; qa2 = qa3; qa3 = ha;
     qb0 = qb1; qb1 = qb2; qb2 = qb3; qb3 = hb;
@@ -307,45 +333,46 @@ k_velocity_fwd_tma(const __grid_constant__ Maps<9> maps, Geo g, Fields f, Psi ps
 template <int TX, int R, int MINB>
 static void stress_launch(dim3 grid, cudaStream_t st, const Maps<11> &maps, const Geo &g,
                           const Fields &f, const Psi &ps, int zchunk, int nzc, const SrcArgs &src,
-                          int *status) {
+                          const ShellMap &shell, int *status) {
   constexpr int B = PlaneRing<3, 8, 2, TX, R>::BYTES;
   static std::atomic<unsigned long long> smem_set{0};
   set_smem_once(k_stress_fwd_tma<TX, R, MINB>, B, smem_set);
   k_stress_fwd_tma<TX, R, MINB><<<grid, dim3(32, TX), B, st>>>(maps, g, f, ps, zchunk, nzc, src,
-                                                              status);
+                                                              shell, status);
 }
 
 template <int TX, int R, int MINB>
 static void velocity_launch(dim3 grid, cudaStream_t st, const Maps<9> &maps, const Geo &g,
-                            const Fields &f, const Psi &ps, int zchunk, int nzc, int *status) {
+                            const Fields &f, const Psi &ps, int zchunk, int nzc,
+                            const RecFuse &rec, int *status) {
   constexpr int B = PlaneRing<5, 4, 1, TX, R>::BYTES;
   static std::atomic<unsigned long long> smem_set{0};
   set_smem_once(k_velocity_fwd_tma<TX, R, MINB>, B, smem_set);
   k_velocity_fwd_tma<TX, R, MINB><<<grid, dim3(32, TX), B, st>>>(maps, g, f, ps, zchunk, nzc,
-                                                                status);
+                                                                rec, status);
 }
 
 int fwd_tma_tile(int cfg) { return cfg == 3 ? 8 : 4; }
 
 void launch_stress_fwd_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<11> &maps,
                            const Geo &g, const Fields &f, const Psi &ps, int zchunk, int nzc,
-                           const SrcArgs &src, int *status) {
+                           const SrcArgs &src, const ShellMap &shell, int *status) {
   switch (cfg) {
-    case 1: stress_launch<4, 3, 7>(grid, st, maps, g, f, ps, zchunk, nzc, src, status); break;
-    case 2: stress_launch<4, 4, 6>(grid, st, maps, g, f, ps, zchunk, nzc, src, status); break;
-    case 3: stress_launch<8, 4, 1>(grid, st, maps, g, f, ps, zchunk, nzc, src, status); break;
-    default: stress_launch<4, 4, 1>(grid, st, maps, g, f, ps, zchunk, nzc, src, status); break;
+    case 1: stress_launch<4, 3, 7>(grid, st, maps, g, f, ps, zchunk, nzc, src, shell, status); break;
+    case 2: stress_launch<4, 4, 6>(grid, st, maps, g, f, ps, zchunk, nzc, src, shell, status); break;
+    case 3: stress_launch<8, 4, 1>(grid, st, maps, g, f, ps, zchunk, nzc, src, shell, status); break;
+    default: stress_launch<4, 4, 1>(grid, st, maps, g, f, ps, zchunk, nzc, src, shell, status); break;
   }
 }
 
 void launch_velocity_fwd_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<9> &maps,
                              const Geo &g, const Fields &f, const Psi &ps, int zchunk, int nzc,
-                             int *status) {
+                             const RecFuse &rec, int *status) {
   switch (cfg) {
-    case 1: velocity_launch<4, 3, 7>(grid, st, maps, g, f, ps, zchunk, nzc, status); break;
-    case 2: velocity_launch<4, 4, 6>(grid, st, maps, g, f, ps, zchunk, nzc, status); break;
-    case 3: velocity_launch<8, 4, 1>(grid, st, maps, g, f, ps, zchunk, nzc, status); break;
-    default: velocity_launch<4, 4, 1>(grid, st, maps, g, f, ps, zchunk, nzc, status); break;
+    case 1: velocity_launch<4, 3, 7>(grid, st, maps, g, f, ps, zchunk, nzc, rec, status); break;
+    case 2: velocity_launch<4, 4, 6>(grid, st, maps, g, f, ps, zchunk, nzc, rec, status); break;
+    case 3: velocity_launch<8, 4, 1>(grid, st, maps, g, f, ps, zchunk, nzc, rec, status); break;
+    default: velocity_launch<4, 4, 1>(grid, st, maps, g, f, ps, zchunk, nzc, rec, status); break;
   }
 }
 

@@ -30,6 +30,36 @@ struct RecArgs {
   const long long *trace_off;
   const int *nrec;      // per shot
   int ncell;
+  // Cell lookup for kernels that gather or inject in their own epilogue:
+  // plane[s * nz + z] names a map [nx][py] of unique receiver cells u in
+  // plane z of shot s (-1 elsewhere), or is -1 when the plane holds none;
+  // plane == nullptr: no lookup (separate k_record / k_inject launches).
+  const int *plane;
+  const int *map;
+  int nxpy;
+};
+
+// Boundary-shell save/restore inside the stencil kernels (efwi_fuse.cuh):
+// rows[z * nx + x] is the index of the row's first shell point (bit 30 set
+// when the row holds two runs, [ya0, ya1] and [yb0, yb1], instead of one
+// run [ya0, yb1]) or -1; store is the [9][npts] shell of the current step
+// in the reference's field order (Boundary.cu:59-96); rows == nullptr: no
+// shell work.
+struct ShellMap {
+  const int *rows;
+  float *store;
+  int npts;
+  int ya0, ya1, yb0, yb1;
+};
+
+// Receiver work fused into a launch: the receivers, the time-major trace
+// array (recorded into by the forward velocity kernel at sample `it`, or
+// read as the adjoint source by the reverse velocity kernel) and `it`;
+// a.plane == nullptr: none.
+struct RecFuse {
+  RecArgs a;
+  float *tm;
+  int it;
 };
 
 // One domain of a multi-domain launch (a shot on its own window grid): its
@@ -79,21 +109,30 @@ void launch_rev_stress(int bx, dim3 grid, cudaStream_t st, const Geo &g, const F
 // tile's x extent.
 int fwd_tma_tile(int cfg);
 // K_S maps: halo vz vx vy | point szz sxx syy sxz sxy syz | model lambda mu.
+// With shell.rows set (one shot per launch), the state at the start of the
+// step is stored into shell.store at the shell points.
 void launch_stress_fwd_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<11> &maps,
                            const Geo &g, const Fields &f, const Psi &ps, int zchunk, int nzc,
-                           const SrcArgs &src, int *status);
+                           const SrcArgs &src, const ShellMap &shell, int *status);
 // K_V maps: halo sxz syz sxx sxy syy | point vz vx vy | model buoyancy.
+// With rec.a.plane set, the new velocities of receiver cells are recorded
+// at sample rec.it.
 void launch_velocity_fwd_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<9> &maps,
                              const Geo &g, const Fields &f, const Psi &ps, int zchunk, int nzc,
-                             int *status);
+                             const RecFuse &rec, int *status);
 
-// Reverse sweep with TMA-staged planes (efwi_rev_tma.cu), tile 32 x 4.
+// Reverse sweep with TMA-staged planes (efwi_rev_tma.cu); rev_tma_tile(cfg)
+// is the tile's x extent (4 or 8; the tile is 32 x that).
+int rev_tma_tile(int cfg);
 // K1 maps: halo sxz syz sxx sxy syy asxz asyz asxx asxy asyy aszz |
 //          point vz vx vy avz avx avy | model buoyancy lambda mu grho.
+// With shell.rows set (do_rev), the reverse velocities are restored at the
+// shell points from shell.store; with inj.a.plane set (do_adj), the adjoint
+// source inj.tm at sample inj.it is added to the adjoint velocities.
 void launch_rev_velocity_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<21> &maps,
                              const Geo &g, const Fields &f, const Fields &a, const Psi &ps,
                              float *grho, int zchunk, int nzc, int do_rev, int do_adj,
-                             int *status);
+                             const ShellMap &shell, const RecFuse &inj, int *status);
 // K1 as two launches (cfg 6, 7): reverse half maps halo sxz syz sxx sxy syy |
 // point vz vx vy avz avx avy | model buoyancy rho-image; adjoint half maps
 // halo asxz asyz asxx asxy asyy aszz | point avz avx avy | model buoyancy
@@ -101,13 +140,16 @@ void launch_rev_velocity_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<21>
 void launch_rev_velocity_split_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<13> &rev_maps,
                                    const Maps<12> &adj_maps, const Geo &g, const Fields &f,
                                    const Fields &a, const Psi &ps, float *grho, int zchunk,
-                                   int nzc, int do_rev, int do_adj, int *status);
+                                   int nzc, int do_rev, int do_adj, const ShellMap &shell,
+                                   const RecFuse &inj, int *status);
 // K2 maps: halo vz vx vy avz avx avy | point szz sxx syy sxz sxy syz aszz
 //          asxx asyy asxz asxy asyz | model lambda mu buoyancy glam gmu.
+// With shell.rows set (do_rev), the reverse stresses are restored at the
+// shell points from shell.store.
 void launch_rev_stress_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<23> &maps,
                            const Geo &g, const Fields &f, const Fields &a, const Psi &ps,
                            float *glam, float *gmu, int zchunk, int nzc, int do_rev, int do_adj,
-                           const SrcArgs &src, int *status);
+                           const SrcArgs &src, const ShellMap &shell, int *status);
 
 __global__ void k_prep_buoyancy(const float *rho, float *buoy, int nz, int nx, int ny, int py);
 __global__ void k_window_slice(const float *src, float *dst, int nz, int nx, int pyg, int x0,

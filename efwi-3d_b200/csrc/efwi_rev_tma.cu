@@ -11,7 +11,14 @@
 //          z queues: vz vx vy avz avx avy
 // Restated reference kernels: velocity.cu:102-131, stress.cu:103-135,
 // velocity_adj.cu:59-144, stress_adj.cu:52-142.
+//
+// Fused epilogues (efwi_fuse.cuh): K1 restores the reverse velocities at
+// the boundary-shell points (to_bnd of the velocities) and adds the adjoint
+// source at the receiver cells to the adjoint velocities (res_injection);
+// K2 restores the reverse stresses at the shell points.  Values written are
+// those the separate kernels would leave, bit for bit.
 #include "efwi_common.cuh"
+#include "efwi_fuse.cuh"
 #include "efwi_kernels.h"
 #include "efwi_tma.cuh"
 
@@ -82,7 +89,8 @@ struct K1L {
 template <int TX, int R, int MINB, int MODE>
 __global__ void __launch_bounds__(32 * TX, MINB)
 k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Fields f, Fields a,
-                   Psi ps, float *grho, int zchunk, int nzc, int do_rev, int do_adj, int *status) {
+                   Psi ps, float *grho, int zchunk, int nzc, int do_rev, int do_adj,
+                   ShellMap shell, RecFuse inj, int *status) {
   using L = K1L<MODE>;
   using Ring = PlaneRing<L::NH, L::NP, L::NM, TX, R>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -149,12 +157,29 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
         }
       }
     }
+    // fused epilogue operands of this plane, loaded before the wait so that
+    // their latency overlaps it: the stored shell velocities (to_bnd) and the
+    // receiver map index (res_injection)
+    int sk = -1;
+    float rvz = 0.f, rvx = 0.f, rvy = 0.f;
+    if (L::REV && shell.rows && act) {
+      sk = shell_index(shell, shell.rows[z * nx + x], y);
+      if (sk >= 0) {
+        const int n = shell.npts;
+        rvz = shell.store[6 * n + sk]; rvx = shell.store[7 * n + sk];
+        rvy = shell.store[8 * n + sk];
+      }
+    }
+    const int rmap = (L::ADJ && inj.a.plane) ? inj.a.plane[z] : -1;
     const bool got = ring.wait(q);
     if (act && got) {
       const float b = ring.point(q, L::MB)[pt];
       const float avz0 = ring.point(q, L::PA)[pt], avx0 = ring.point(q, L::PA + 1)[pt],
                   avy0 = ring.point(q, L::PA + 2)[pt];
-      if (L::REV && do_rev && xin && yin && z >= np && z <= nz - 1 - np) {
+      if (L::REV && do_rev) {
+        const bool inr = xin && yin && z >= np && z <= nz - 1 - np;
+        float nvz = 0.f, nvx = 0.f, nvy = 0.f;
+        if (inr) {
         const BoxView bsxz{ring.halo(q, 0) + off}, bsyz{ring.halo(q, 1) + off},
             bsxx{ring.halo(q, 2) + off}, bsxy{ring.halo(q, 3) + off}, bsyy{ring.halo(q, 4) + off};
         const float sxy_0 = bsxy.c(), sxy_xm1 = bsxy.x(-1);
@@ -167,12 +192,16 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
         const float dy_ = dminus(syz.a, syz.b, syz.c, syz.d) * idz +
                           (EFWI_C1 * (sxy_0 - sxy_xm1) - EFWI_C2 * (sxy_xm1 - bsxy.x(-2))) * idx +
                           dplus(bsyy.y(-1), bsyy.c(), bsyy.y(1), bsyy.y(2)) * idy;
-        f.vz[i] = ring.point(q, 0)[pt] - dz_ * b * dt;
-        f.vx[i] = ring.point(q, 1)[pt] - dx_ * b * dt;
-        f.vy[i] = ring.point(q, 2)[pt] - dy_ * b * dt;
+        nvz = ring.point(q, 0)[pt] - dz_ * b * dt;
+        nvx = ring.point(q, 1)[pt] - dx_ * b * dt;
+        nvy = ring.point(q, 2)[pt] - dy_ * b * dt;
         const float nb2 = -(b * b);
         grho[i] = ring.point(q, L::MG)[pt] -
                     (avz0 * dz_ * dt * nb2 + avx0 * dx_ * dt * nb2 + avy0 * dy_ * dt * nb2);
+        }
+        // to_bnd: the shell points take the stored velocities of the step
+        if (sk >= 0) { nvz = rvz; nvx = rvx; nvy = rvy; }
+        if (inr || sk >= 0) { f.vz[i] = nvz; f.vx[i] = nvx; f.vy[i] = nvy; }
       }
       if (L::ADJ && do_adj) {
         const BoxView basxz{ring.halo(q, L::HA) + off}, basyz{ring.halo(q, L::HA + 1) + off},
@@ -181,6 +210,7 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
         const bool zs = slab_s(z, nz, np);
         const Coef cz = coef(g.cz, nz, z);
         const float l = ring.point(q, L::ML)[pt], u = ring.point(q, L::MM)[pt], l2u = l + 2.0f * u;
+        float nax, naz, nay;  // the new adjoint velocities (before res_injection)
         {  // adjoint vx
           const float dszz_dx = -dplus(baszz.x(-1), aszz.b, baszz.x(1), baszz.x(2)) * idx;
           const float dsxx_dx = -dplus(basxx.x(-1), asxx.b, basxx.x(1), basxx.x(2)) * idx;
@@ -194,7 +224,7 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
           if (zs) acc += cz.ah * (nzm(g, psz + PSI_VB1 * g.slab_z, z, x, y) * idz);
           if (ys) acc += cy.ah * (nym(g, psy + PSI_VB2 * g.slab_y, z, x, y) * idy);
           const float v = avx0 + acc;
-          a.vx[i] = v;
+          nax = v;
           if (xs) { const long long k = PSI_SAA * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.bh * px[k] + b * v * dt; }
           if (zs) { const long long k = PSI_SAB1 * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.b * pz[k] + b * v * dt; }
           if (ys) { const long long k = PSI_SAB2 * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.b * py[k] + b * v * dt; }
@@ -212,7 +242,7 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
           if (ys) acc += cy.ah * (nym(g, psy + PSI_VB1 * g.slab_y, z, x, y) * idy);
           if (xs) acc += cx.ah * (nxm(g, psx + PSI_VB1 * g.slab_x, z, x, y) * idx);
           const float v = avz0 + acc;
-          a.vz[i] = v;
+          naz = v;
           if (xs) { const long long k = PSI_SAB1 * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.b * px[k] + b * v * dt; }
           if (zs) { const long long k = PSI_SAA * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.bh * pz[k] + b * v * dt; }
           if (ys) { const long long k = PSI_SAB1 * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.b * py[k] + b * v * dt; }
@@ -230,11 +260,16 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
           if (xs) acc += cx.ah * (nxm(g, psx + PSI_VB2 * g.slab_x, z, x, y) * idx);
           if (zs) acc += cz.ah * (nzm(g, psz + PSI_VB2 * g.slab_z, z, x, y) * idz);
           const float v = avy0 + acc;
-          a.vy[i] = v;
+          nay = v;
           if (xs) { const long long k = PSI_SAB2 * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.b * px[k] + b * v * dt; }
           if (zs) { const long long k = PSI_SAB2 * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.bh * pz[k] + b * v * dt; }
           if (ys) { const long long k = PSI_SAA * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.b * py[k] + b * v * dt; }
         }
+        if (rmap >= 0) {  // res_injection after the adjoint update
+          const int ur = inj.a.map[(long long)rmap * inj.a.nxpy + x * g.sx + y];
+          if (ur >= 0) inject_cell(inj.a, inj.tm, inj.it, ur, naz, nax, nay);
+        }
+        a.vx[i] = nax; a.vz[i] = naz; a.vy[i] = nay;
       }
     }
     szz.shift(h0); sxz.shift(h1); syz.shift(h2); aszz.shift(h3);
@@ -254,7 +289,7 @@ template <int TX, int R, int MINB>
 __global__ void __launch_bounds__(32 * TX, MINB)
 k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields a, Psi ps,
                  float *glam, float *gmu, int zchunk, int nzc, int do_rev, int do_adj,
-                 SrcArgs src, int *status) {
+                 SrcArgs src, ShellMap shell, int *status) {
   using Ring = PlaneRing<6, 17, 5, TX, R>;
   extern __shared__ __align__(128) unsigned char smem[];
   Ring ring;
@@ -310,6 +345,17 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
         prefetch_l2(a.vz + i + 3 * sz); prefetch_l2(a.vx + i + 4 * sz); prefetch_l2(a.vy + i + 4 * sz);
       }
     }
+    // the stored shell stresses of this plane (to_bnd), loaded before the
+    // wait so that their latency overlaps it
+    int sk = -1;
+    float rst[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (shell.rows && act) {
+      sk = shell_index(shell, shell.rows[z * nx + x], y);
+      if (sk >= 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) rst[k] = shell.store[k * shell.npts + sk];
+      }
+    }
     const bool got = ring.wait(q);
     if (act && got) {
       const BoxView bvz{ring.halo(q, 0) + off}, bvx{ring.halo(q, 1) + off},
@@ -329,7 +375,9 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
           sxx = (float)((double)sxx - am);
           syy = (float)((double)syy - am);
         }
-        if (xin && yin && z >= np && z <= nz - 1 - np) {
+        const bool inr = xin && yin && z >= np && z <= nz - 1 - np;
+        float nsxz = 0.f, nsxy = 0.f, nsyz = 0.f;
+        if (inr) {
           const float ezz = dminus(vz.a, vz.b, vz.c, vz.d) * idz;
           const float exx = dminus(bvx.x(-2), bvx.x(-1), vx.b, bvx.x(1)) * idx;
           const float eyy = dminus(bvy.y(-2), bvy.y(-1), vy.b, bvy.y(1)) * idy;
@@ -342,15 +390,20 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
           const float dvz_dy = dplus(bvz.y(-1), vz.c, bvz.y(1), bvz.y(2)) * idy;
           const float dvy_dx = dplus(bvy.x(-1), vy.b, bvy.x(1), bvy.x(2)) * idx;
           const float dvy_dz = dplus(vy.a, vy.b, vy.c, vy.d) * idz;
-          f.sxz[i] = ring.point(q, 3)[pt] - u * (dvx_dz + dvz_dx) * dt;
-          f.sxy[i] = ring.point(q, 4)[pt] - u * (dvx_dy + dvy_dx) * dt;
-          f.syz[i] = ring.point(q, 5)[pt] - u * (dvy_dz + dvz_dy) * dt;
+          nsxz = ring.point(q, 3)[pt] - u * (dvx_dz + dvz_dx) * dt;
+          nsxy = ring.point(q, 4)[pt] - u * (dvx_dy + dvy_dx) * dt;
+          nsyz = ring.point(q, 5)[pt] - u * (dvy_dz + dvz_dy) * dt;
           glam[i] = ring.point(q, 15)[pt] - (azz0 + axx0 + ayy0) * (ezz + exx + eyy) * dt;
           gmu[i] = ring.point(q, 16)[pt] -
                      (2.0f * azz0 * ezz + 2.0f * axx0 * exx + 2.0f * ayy0 * eyy +
                       axz0 * (dvx_dz + dvz_dx) + ayz0 * (dvy_dz + dvz_dy) +
                       axy0 * (dvy_dx + dvx_dy)) * dt;
         }
+        // to_bnd: the shell points take the stored stresses of the step
+        if (sk >= 0) {
+          szz = rst[0]; nsxz = rst[1]; sxx = rst[2]; syy = rst[3]; nsxy = rst[4]; nsyz = rst[5];
+        }
+        if (inr || sk >= 0) { f.sxz[i] = nsxz; f.sxy[i] = nsxy; f.syz[i] = nsyz; }
         f.szz[i] = szz; f.sxx[i] = sxx; f.syy[i] = syy;
       }
       if (do_adj) {
@@ -420,43 +473,47 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
 }
 
 
-// Launch configurations of the reverse TMA kernels (32 x 4 tiles):
-// (ring depth, minimum resident CTAs per SM).
-template <int R, int MINB, int MODE = 0>
+// Launch configurations of the reverse TMA kernels (32 x 4 tiles): (ring
+// depth, minimum resident CTAs per SM).  32 x 8 tiles were measured slower
+// (0.227 / 0.243 ms against 0.198 / 0.200 ms per launch at 152^3).
+int rev_tma_tile(int) { return 4; }
+template <int R, int MINB, int MODE = 0, int TX = 4>
 static void revv_launch(dim3 grid, cudaStream_t st, const Maps<K1L<MODE>::N> &maps, const Geo &g,
                         const Fields &f, const Fields &a, const Psi &ps, float *grho, int zchunk,
-                        int nzc, int do_rev, int do_adj, int *status) {
+                        int nzc, int do_rev, int do_adj, const ShellMap &shell,
+                        const RecFuse &inj, int *status) {
   using L = K1L<MODE>;
-  constexpr int B = PlaneRing<L::NH, L::NP, L::NM, 4, R>::BYTES;
+  constexpr int B = PlaneRing<L::NH, L::NP, L::NM, TX, R>::BYTES;
   static std::atomic<unsigned long long> smem_set{0};
-  set_smem_once(k_rev_velocity_tma<4, R, MINB, MODE>, B, smem_set);
-  k_rev_velocity_tma<4, R, MINB, MODE><<<grid, dim3(32, 4), B, st>>>(
-      maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status);
+  set_smem_once(k_rev_velocity_tma<TX, R, MINB, MODE>, B, smem_set);
+  k_rev_velocity_tma<TX, R, MINB, MODE><<<grid, dim3(32, TX), B, st>>>(
+      maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, shell, inj, status);
 }
 
-template <int R, int MINB>
+template <int R, int MINB, int TX = 4>
 static void revs_launch(dim3 grid, cudaStream_t st, const Maps<23> &maps, const Geo &g,
                         const Fields &f, const Fields &a, const Psi &ps, float *glam, float *gmu,
                         int zchunk, int nzc, int do_rev, int do_adj, const SrcArgs &src,
-                        int *status) {
-  constexpr int B = PlaneRing<6, 17, 5, 4, R>::BYTES;
+                        const ShellMap &shell, int *status) {
+  constexpr int B = PlaneRing<6, 17, 5, TX, R>::BYTES;
   static std::atomic<unsigned long long> smem_set{0};
-  set_smem_once(k_rev_stress_tma<4, R, MINB>, B, smem_set);
-  k_rev_stress_tma<4, R, MINB><<<grid, dim3(32, 4), B, st>>>(maps, g, f, a, ps, glam, gmu, zchunk,
-                                                            nzc, do_rev, do_adj, src, status);
+  set_smem_once(k_rev_stress_tma<TX, R, MINB>, B, smem_set);
+  k_rev_stress_tma<TX, R, MINB><<<grid, dim3(32, TX), B, st>>>(maps, g, f, a, ps, glam, gmu, zchunk,
+                                                            nzc, do_rev, do_adj, src, shell,
+                                                            status);
 }
 
 void launch_rev_velocity_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<21> &maps,
                              const Geo &g, const Fields &f, const Fields &a, const Psi &ps,
                              float *grho, int zchunk, int nzc, int do_rev, int do_adj,
-                             int *status) {
+                             const ShellMap &shell, const RecFuse &inj, int *status) {
   switch (cfg) {
-    case 1: revv_launch<2, 4>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
-    case 2: revv_launch<3, 4>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
-    case 3: revv_launch<2, 1>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
-    case 4: revv_launch<2, 5>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
-    case 5: revv_launch<2, 6>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
-    default: revv_launch<3, 1>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, status); break;
+    case 1: revv_launch<2, 4>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, shell, inj, status); break;
+    case 2: revv_launch<3, 4>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, shell, inj, status); break;
+    case 3: revv_launch<2, 1>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, shell, inj, status); break;
+    case 4: revv_launch<2, 5>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, shell, inj, status); break;
+    case 5: revv_launch<2, 6>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, shell, inj, status); break;
+    default: revv_launch<3, 1>(grid, st, maps, g, f, a, ps, grho, zchunk, nzc, do_rev, do_adj, shell, inj, status); break;
   }
 }
 
@@ -465,29 +522,30 @@ void launch_rev_velocity_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<21>
 void launch_rev_velocity_split_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<13> &rev_maps,
                                    const Maps<12> &adj_maps, const Geo &g, const Fields &f,
                                    const Fields &a, const Psi &ps, float *grho, int zchunk,
-                                   int nzc, int do_rev, int do_adj, int *status) {
+                                   int nzc, int do_rev, int do_adj, const ShellMap &shell,
+                                   const RecFuse &inj, int *status) {
   if (cfg == 7) {
-    if (do_rev) revv_launch<3, 8, 1>(grid, st, rev_maps, g, f, a, ps, grho, zchunk, nzc, 1, 0, status);
-    if (do_adj) revv_launch<3, 4, 2>(grid, st, adj_maps, g, f, a, ps, grho, zchunk, nzc, 0, 1, status);
+    if (do_rev) revv_launch<3, 8, 1>(grid, st, rev_maps, g, f, a, ps, grho, zchunk, nzc, 1, 0, shell, RecFuse{}, status);
+    if (do_adj) revv_launch<3, 4, 2>(grid, st, adj_maps, g, f, a, ps, grho, zchunk, nzc, 0, 1, ShellMap{}, inj, status);
   } else {
-    if (do_rev) revv_launch<2, 8, 1>(grid, st, rev_maps, g, f, a, ps, grho, zchunk, nzc, 1, 0, status);
-    if (do_adj) revv_launch<2, 5, 2>(grid, st, adj_maps, g, f, a, ps, grho, zchunk, nzc, 0, 1, status);
+    if (do_rev) revv_launch<2, 8, 1>(grid, st, rev_maps, g, f, a, ps, grho, zchunk, nzc, 1, 0, shell, RecFuse{}, status);
+    if (do_adj) revv_launch<2, 5, 2>(grid, st, adj_maps, g, f, a, ps, grho, zchunk, nzc, 0, 1, ShellMap{}, inj, status);
   }
 }
 
 void launch_rev_stress_tma(int cfg, dim3 grid, cudaStream_t st, const Maps<23> &maps,
                            const Geo &g, const Fields &f, const Fields &a, const Psi &ps,
                            float *glam, float *gmu, int zchunk, int nzc, int do_rev, int do_adj,
-                           const SrcArgs &src, int *status) {
+                           const SrcArgs &src, const ShellMap &shell, int *status) {
   switch (cfg) {
-    case 1: revs_launch<2, 5>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
-    case 2: revs_launch<3, 4>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
-    case 3: revs_launch<2, 1>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
-    case 4: revs_launch<2, 6>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
-    case 5: revs_launch<2, 7>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
-    case 6: revs_launch<2, 5>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
-    case 7: revs_launch<3, 4>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
-    default: revs_launch<3, 1>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, status); break;
+    case 1: revs_launch<2, 5>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, shell, status); break;
+    case 2: revs_launch<3, 4>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, shell, status); break;
+    case 3: revs_launch<2, 1>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, shell, status); break;
+    case 4: revs_launch<2, 6>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, shell, status); break;
+    case 5: revs_launch<2, 7>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, shell, status); break;
+    case 6: revs_launch<2, 5>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, shell, status); break;
+    case 7: revs_launch<3, 4>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, shell, status); break;
+    default: revs_launch<3, 1>(grid, st, maps, g, f, a, ps, glam, gmu, zchunk, nzc, do_rev, do_adj, src, shell, status); break;
   }
 }
 

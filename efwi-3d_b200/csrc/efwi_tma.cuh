@@ -88,20 +88,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   return true;
 }
 
-// 3-D tiled bulk tensor load of one box into shared memory (no multicast).
 // Raises a kernel's dynamic shared-memory limit once per device: the
 // attribute belongs to the device's context, so a process that drives
-// several GPUs sets it on each (bit d of `done` stands for device d).
+// several GPUs sets it on each (bit d of `done` stands for device d).  The
+// bit is set only when the call succeeded; a failure stays pending as the
+// runtime's last error, which the launch wrapper's check reports for the
+// launch that needed the attribute.
 template <class K>
 inline void set_smem_once(K kernel, int bytes, std::atomic<unsigned long long> &done) {
   int dev = 0;
-  cudaGetDevice(&dev);
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
   const unsigned long long bit = 1ull << (dev & 63);
   if (done.load(std::memory_order_acquire) & bit) return;
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  done.fetch_or(bit, std::memory_order_acq_rel);
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) ==
+      cudaSuccess)
+    done.fetch_or(bit, std::memory_order_acq_rel);
 }
 
+// 3-D tiled bulk tensor load of one box into shared memory (no multicast).
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
                                             int c0, int c1, int c2) {
   asm volatile(
@@ -171,7 +175,13 @@ struct PlaneRing {
 };
 
 // Leaves a CTA whose pipeline timed out: records the status, waits (bounded)
-// for the copies it still has in flight, then every thread returns.
+// for the copies it still has in flight, then every thread returns.  Best
+// effort: if that wait runs out as well, a copy may still land in shared
+// memory after the CTA has left (in another CTA's buffers), so once the
+// status word reads EFWI_STATUS_TIMEOUT the host reports the whole call as
+// failed and none of its device results may be used; every call zeroes the
+// state, memory variables, images and traces it uses before its first
+// kernel, so no stale value carries into the next call.
 template <class Ring>
 __device__ __forceinline__ void ring_abort(Ring &ring, int q, int nq, int R, int tid, int *status) {
   if (tid == 0) {

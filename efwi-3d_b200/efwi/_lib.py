@@ -66,6 +66,7 @@ _SIGS = {
     "efwi_version": (C.c_char_p, []),
     "efwi_set_options": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
     "efwi_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "efwi_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "efwi_set_tuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
     "efwi_set_nt_limit": (C.c_int, [C.c_void_p, C.c_int]),
     "efwi_set_lanes": (C.c_int, [C.c_void_p, C.c_int]),

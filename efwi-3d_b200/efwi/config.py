@@ -152,3 +152,31 @@ def write_shot_data(data_dir: str, shot_id: int, traces: np.ndarray, prefix: str
     for c, comp in enumerate("xyz"):
         np.ascontiguousarray(traces[c], np.float32).tofile(
             os.path.join(data_dir, f"{prefix}{comp}{shot_id}.bin"))
+
+
+def write_problem(dirpath: str, grid, shots, traces=None, shot_ids=None) -> str:
+    """Writes the para JSON, the survey JSON and (optionally) observed data
+    Shot_{x,y,z}{id}.bin of a problem into `dirpath`, in the formats the
+    reference reads (Parameter.cpp, Src_Rec.cu, libCUFD.cu:277-279): padded
+    sizes in the para file, model-relative indices in the survey.  `traces`
+    is a list of [3][nrec][nt] arrays of the shots `shot_ids`.  Returns the
+    para file's path."""
+    import fwi_utils as ft
+    para = os.path.join(dirpath, "para_file.json")
+    survey = os.path.join(dirpath, "survey_file.json")
+    data = os.path.join(dirpath, "Data")
+    g = grid
+    ft.paraGen_3d(g.nz, g.nx, g.ny, g.dz, g.dx, g.dy, g.nt, g.dt, g.f0, g.npml, para, survey, data)
+    sv = {"nShots": len(shots)}
+    for k, s in enumerate(shots):
+        sv[f"shot{k}"] = {"z_src": int(s.src[0]) - g.npml, "x_src": int(s.src[1]) - g.npml,
+                          "y_src": int(s.src[2]) - g.npml, "nrec": s.nrec,
+                          "z_rec": (np.asarray(s.z_rec) - g.npml).tolist(),
+                          "x_rec": (np.asarray(s.x_rec) - g.npml).tolist(),
+                          "y_rec": (np.asarray(s.y_rec) - g.npml).tolist()}
+    with open(survey, "w") as fp:
+        json.dump(sv, fp)
+    if traces is not None:
+        for k, t in zip(shot_ids, traces):
+            write_shot_data(data, k, np.asarray(t))
+    return para

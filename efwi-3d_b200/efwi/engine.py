@@ -109,6 +109,11 @@ class Propagator:
         check(self._h, self._L.efwi_set_options(self._h, int(if_win), int(tile_bx), int(zchunk),
                                                 int(max_batch)))
 
+    def set_graphs(self, on: bool) -> None:
+        """Time loops as CUDA graphs replayed across shots and calls (default
+        on); off launches every kernel from the host (same results)."""
+        check(self._h, self._L.efwi_set_graphs(self._h, int(bool(on))))
+
     def set_variant(self, variant: int) -> None:
         """1: TMA-staged stencil planes (default); 0: L1-served stencils."""
         check(self._h, self._L.efwi_set_variant(self._h, int(variant)))

@@ -75,6 +75,16 @@ int efwi_set_options(EfwiHandle *h, int if_win, int tile_bx, int zchunk, int max
  * reference counterpart (the reference has one plain kernel per update). */
 int efwi_set_variant(EfwiHandle *h, int variant);
 
+/* CUDA graphs of the time loops (default on): the forward time loop of a
+ * batch and the reverse time loop of a reference-mode gradient shot are
+ * captured once and replayed while their launch parameters (buffers,
+ * tensor maps, tuning, time axis) are unchanged, across shots and calls.
+ * on = 0 launches them one by one (results are bitwise the same).  Runs with
+ * kernel-event sampling (efwi_profile) launch eagerly.  No reference
+ * counterpart (the reference launches about 25 kernels per step from the
+ * host, libCUFD.cu:312-354, 532-612). */
+int efwi_set_graphs(EfwiHandle *h, int on);
+
 /* Launch configuration of the TMA kernels (the autotuner's knobs; results
  * do not depend on them): fwd_cfg in 0..3 and rev_cfg in 0..7 select tile,
  * ring depth and occupancy target (rev_cfg 6, 7 run the reverse-velocity
@@ -225,7 +235,10 @@ int efwi_set_scratch(EfwiHandle *h, float *syn_w, float *obs_w, float *res);
  * until exit); requests needing more than that many 32 x 32 tiles
  * (3 * ceil(nt/32) * ceil(nrec/32)) return EFWI_ERR_TOO_LARGE.  The first
  * call on a device looks up the array's address and should come before any
- * stream capture.  Calls that overlap on the GPU race on the array. */
+ * stream capture.  Calls that overlap on the GPU race on the array.  The
+ * address is kept per device for the life of the process: it assumes the
+ * device's primary context is never destroyed (after cudaDeviceReset the
+ * library must be reloaded before this entry point is called again). */
 #define EFWI_NOALLOC_MAX_PARTIALS 65536
 int efwi_misfit_noalloc(int nrec, int nt, float dt, int if_win, const float *win_start,
                         const float *win_end, const float *weights, float src_weight,
