@@ -58,7 +58,9 @@ def parse():
                     help="time steps of each sample of --impl reference (one per step)")
     ap.add_argument("--lanes", type=int, default=2,
                     help="shots of the gradient that run concurrently (efwi_set_lanes)")
-    ap.add_argument("--tile-bx", type=int, default=4)
+    ap.add_argument("--tile-bx", type=int, default=None,
+                    help="x rows of the exact adjoint kernels' tile (default 8) and of the "
+                         "L1 stencils (default 4)")
     ap.add_argument("--zchunk", type=int, default=8)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--mode", default="reference", choices=["reference", "exact"],
@@ -336,7 +338,7 @@ def run_case(a):
     from efwi import synthetic
     from efwi.engine import Propagator
     p = synthetic.config2(nt=a.nt, nshot=1, n=a.n)
-    P = Propagator(p.grid, tile_bx=a.tile_bx)
+    P = Propagator(p.grid, tile_bx=a.tile_bx or (8 if a.case == "exact" else 4))
     P.set_tuning(*[int(v) for v in a.tuning.split(",")])
     P.set_survey(p.shots, p.stf)
     P.set_model(*[torch.from_numpy(x) for x in p.params("true")])
@@ -444,6 +446,9 @@ def run_windows(a):
     lam, mu, rh = synthetic.elastic_params(vp, vs, rho, grid.npml)
     P.set_model(torch.from_numpy(lam), torch.from_numpy(mu), torch.from_numpy(rh))
     ids = list(range(len(shots)))
+    if a.case == "windows-gradient":
+        run_window_gradient(a, P, grid, shots, wins, (lam, mu, rh))
+        return
     tune = autotune_windows(P, ids, wins)
     for _ in range(max(a.warmup, 1)):
         P.forward_windows(ids, wins, use_graph=True)
@@ -473,8 +478,43 @@ def run_windows(a):
         "roofline": {"bound": "hbm", "achieved": bytes_step / (ms * 1e-3) / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": bytes_step / (ms * 1e-3) / 1e9 / peak,
                      "peak_kind": kind, "bytes": "120 N + 48 S per window and step"},
-        "graph": tune["variant"] == "l1", "clocks": clocks}))
+        "graph": True,
+        "graph_form": "one persistent multi-domain launch per half-step, whole time loop in one "
+                      "graph" if tune["variant"] == "l1" else
+                      "per-window TMA launches on 8 streams, one time step captured as a graph "
+                      "(parallel branches) and replayed per step",
+        "clocks": clocks}))
     P.close()
+
+
+def run_window_gradient(a, P, grid, shots, wins, model):
+    """Config 4's windows, one reference-mode gradient of every shot on its
+    window (efwi_gradient_windows) against data of a model 3 % faster;
+    cell-updates/s counted over the windows' cells, as the forward case."""
+    import numpy as np
+    import torch
+    ids = list(range(len(shots)))
+    lam, mu, rh = model
+    P.set_model(*[torch.from_numpy(m * np.float32(1.03)) for m in (lam, mu)],
+                torch.from_numpy(rh))
+    P.set_tuning(1, 8, 4, 4)
+    obs = P.forward(ids)
+    P.set_model(torch.from_numpy(lam), torch.from_numpy(mu), torch.from_numpy(rh))
+    warm = torch.cat([t.reshape(-1) for t in P.split(obs, ids)[:2]])
+    P.gradient_windows(ids[:2], wins[:2], warm)  # window engines, graphs
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    J, gl, gm, gr = P.gradient_windows(ids, wins, obs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cells = [grid.nz * w[2] * w[3] for w in wins]
+    agg = sum(cells) * grid.nt / (ms * 1e-3) / 1e9
+    print(json.dumps({"case": "windows-gradient", "nt": grid.nt, "windows": len(wins),
+                      "misfit": J, "ms_per_call": ms, "aggregate_gcell_per_s": agg,
+                      "mode": "reference", "tuning": "1,8,4,4",
+                      "note": "windows run one after another, each on its own grid"}))
 
 
 def run_refgpu(a):
@@ -538,7 +578,7 @@ def main():
     if a.case == "inversion":
         run_inversion(a)
         return
-    if a.case == "windows":
+    if a.case in ("windows", "windows-gradient"):
         run_windows(a)
         return
     if a.case == "refgpu":
@@ -571,7 +611,8 @@ def main():
     prob = synthetic.config2(nt=a.nt, nshot=a.shots, n=a.n, seed=2 + rank)
     g = prob.grid
     ids = list(range(len(prob.shots)))
-    P = Propagator(g, device=dev, tile_bx=a.tile_bx, zchunk=a.zchunk, max_batch=4)
+    bx = a.tile_bx or (8 if a.mode == "exact" else 4)
+    P = Propagator(g, device=dev, tile_bx=bx, zchunk=a.zchunk, max_batch=4)
     P.set_lanes(a.lanes)
     P.set_checkpoint_budget(int(a.ck_budget * (1 << 30)))
     P.set_survey(prob.shots, prob.stf)
@@ -627,6 +668,7 @@ def main():
         dist.barrier()
     counted = P.profile_read()
     clocks = clk.stop()
+    ck_stats = P.checkpoint_stats() if a.mode == "exact" else None
     # Per-kernel launch times from a separate, untimed pass on one lane (no
     # other shot's kernels share the GPU with the timed launches): every
     # k-th time step of a gradient over the first shots.
@@ -675,6 +717,7 @@ def main():
         import FWI_ops_3d as F
         P.set_lanes(1)  # frees the extra lanes' workspace for the drop-in's own
         F.set_lanes(a.lanes)
+        F.set_tuning(P.tuning)  # the same launch configuration as the timed run
         with tempfile.TemporaryDirectory() as tmp:
             para = write_dropin_files(tmp, prob, P.split(obs, ids), ids)
             lam_h, mu_h, rho_h = (torch.from_numpy(x).pin_memory() for x in prob.params("init"))
@@ -723,8 +766,9 @@ def main():
                                        f" {len(ids)} shots per GPU, nt={g.nt}, {a.mode} gradient",
                            "model_cells": a.n, "padded": g.nz, "shots_per_gpu": len(ids),
                            "nt": g.nt, "mode": a.mode,
-                           "lanes": a.lanes if a.mode == "reference" else 1,
-                           "checkpoints": P.checkpoint_stats() if a.mode == "exact" else None,
+                           "lanes": a.lanes,
+                           "checkpoints": ck_stats,
+                           "checkpoint_budget_gib": a.ck_budget if a.mode == "exact" else None,
                            "l2": "inputs larger than L2 (9 fields x 14 MB per shot + shell store)",
                            "autotune": tune},
                 "roofline": roof, "step_roofline": whole, "cpu_baseline": cpu, "e2e": e2e,

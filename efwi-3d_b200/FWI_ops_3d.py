@@ -31,7 +31,7 @@ from efwi import config as _cfg
 from efwi.autotune import autotune
 from efwi.engine import Propagator
 
-__all__ = ["fwi_ops", "FWIFunction", "FWI_3d", "FWI_obscalc", "set_lanes"]
+__all__ = ["fwi_ops", "FWIFunction", "FWI_3d", "FWI_obscalc", "set_lanes", "set_tuning"]
 
 
 def _mtime(path: str) -> Tuple[float, int]:
@@ -48,6 +48,21 @@ def _mtime(path: str) -> Tuple[float, int]:
 # device memory at the call is left out.
 LANES = 2
 _lanes_by_para: Dict[str, int] = {}
+
+
+# Launch configuration of later sessions: None autotunes on a session's
+# first gradient call; a tuple (fwd_cfg, zchunk_fwd, rev_cfg, zchunk_rev)
+# is used as it is (efwi_set_tuning).
+TUNING: Optional[Tuple[int, int, int, int]] = None
+
+
+def set_tuning(tuning: Optional[Tuple[int, int, int, int]]) -> None:
+    """Fixes the stencil launch configuration of the sessions (None: the
+    autotuner picks it on a session's first gradient call)."""
+    global TUNING
+    TUNING = None if tuning is None else tuple(int(v) for v in tuning)
+    for s in _sessions.values():
+        s.tuned = False
 
 
 def set_lanes(n: int, para_fname: Optional[str] = None) -> None:
@@ -256,6 +271,9 @@ class _FwiOps:
                     s.check_ids(shards[i])
                     s.prop.set_model(Lambda, Mu, Den)
                     obs = s.observed(shards[i])
+                    if not s.tuned and TUNING is not None:
+                        s.prop.set_tuning(*TUNING)
+                        s.tuned = True
                     if not s.tuned:
                         # launch shapes timed once per session on the real grid
                         nt = s.para.grid.nt

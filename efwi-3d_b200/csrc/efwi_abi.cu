@@ -174,7 +174,12 @@ struct EfwiHandle {
   // exact gradient: checkpoint slots and the two adjoint memory-variable sets
   DevBuf ckpt, apsi;
   // shot windows: per-domain volumes and tables; stream for graph capture
-  DevBuf wvol, wtab;
+  DevBuf wvol, wtab, wstep;
+  // windowed gradients: one sub-handle per window shape (its own grid and
+  // C-PML), scratch for the window's observed data and images
+  std::map<std::pair<int, int>, EfwiHandle *> wsub;
+  DevBuf wobs, wimg, wsel;
+  std::vector<float> stf_host;  // untapered source-time functions [nshot][nt]
   cudaStream_t cap_stream = nullptr;
   // shot windows on the TMA kernels: window groups run on their own streams
   cudaStream_t wst[8] = {};
@@ -346,6 +351,36 @@ bool shell_rows(const EfwiGrid &g, int py, const std::vector<int> &pts, std::vec
   }
   return named == (long long)pts.size();
 }
+
+// out[c][j][t] = obs[c][sel[j]][t]: the observed data of the receivers
+// that lie inside a window (traces layout [3][nrec][nt]).
+__global__ void k_gather_rows(const float *obs, const int *sel, int nsel, int nrec, int nt,
+                              float *out) {
+  const long long n = 3LL * nsel * nt;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i % nt);
+    const long long cj = i / nt;
+    const int j = (int)(cj % nsel), c = (int)(cj / nsel);
+    out[i] = obs[((long long)c * nrec + sel[j]) * nt + t];
+  }
+}
+
+// g[z][x0 + x][y0 + y] += w[z][x][y] (caller layouts, no pitch).
+__global__ void k_window_add(float *g, const float *w, int nz, int nx, int ny, int x0, int y0,
+                             int nxw, int nyw) {
+  const long long n = (long long)nz * nxw * nyw;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % nyw);
+    const long long zx = i / nyw;
+    const int x = (int)(zx % nxw), z = (int)(zx / nxw);
+    g[((long long)z * nx + x0 + x) * ny + y0 + y] += w[i];
+  }
+}
+
+// Step counter of a time loop replayed from a graph of one step.
+__global__ void k_step_advance(int *it) { if (threadIdx.x == 0 && blockIdx.x == 0) ++*it; }
 
 __global__ void k_add(float *__restrict__ dst, const float *__restrict__ src, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -1041,7 +1076,7 @@ int make_window_maps(EfwiHandle *h, const Domain &d, int bxf, FwdMaps *maps) {
 // GPU; the other streams fill the tails between launches.
 int window_loop_tma(EfwiHandle *h, const std::vector<Domain> &dom, const std::vector<int> &rec_dom,
                     const Domain *ddom, const int *drd, const int *drc, const int *drr,
-                    long long *dsrc, float *ttm, int ntl, cudaStream_t st) {
+                    long long *dsrc, float *ttm, int ntl, bool use_graph, cudaStream_t st) {
   const int n = (int)dom.size();
   int rc = status_reset(h, st);
   if (rc) return rc;
@@ -1085,12 +1120,13 @@ int window_loop_tma(EfwiHandle *h, const std::vector<Domain> &dom, const std::ve
     grids[k] = dim3((g.ny + 31) / 32, (g.nx + bxf - 1) / bxf, nzcs[k]);
   }
   long long nrec_launch = 0;
-  for (int it = 0; it <= ntl - 2; ++it) {
+  // one time step of every group (it_dev: the step read from device memory)
+  auto step = [&](int it, const int *it_dev) {
     for (int g = 0; g < G; ++g) {
       cudaStream_t s = h->wst[g];
       for (int k = gbeg[g]; k < gbeg[g + 1]; ++k) {
         const Domain &d = dom[k];
-        const SrcArgs src{dsrc + k, d.stf, nt, it};
+        const SrcArgs src{dsrc + k, d.stf, nt, it, it_dev};
         launch_stress_fwd_tma(h->fcfg, grids[k], s, maps[k].s, d.g, d.f, d.ps, h->zchunk, nzcs[k],
                               src, ShellMap{}, status);
         launch_velocity_fwd_tma(h->fcfg, grids[k], s, maps[k].v, d.g, d.f, d.ps, h->zchunk,
@@ -1099,16 +1135,53 @@ int window_loop_tma(EfwiHandle *h, const std::vector<Domain> &dom, const std::ve
       const int r0 = rstart[gbeg[g]], r1 = rstart[gbeg[g + 1]];
       if (r1 > r0) {
         k_record_multi<<<(r1 - r0 + 127) / 128, 128, 0, s>>>(ddom, drd + r0, drc + r0, drr + r0,
-                                                               r1 - r0, ttm, it + 1);
+                                                               r1 - r0, ttm, it + 1, it_dev);
         ++nrec_launch;
       }
     }
-  }
-  for (int g = 0; g < G; ++g) {
-    CK_CUDA(h, cudaEventRecord(h->wev[g], h->wst[g]));
-    CK_CUDA(h, cudaStreamWaitEvent(st, h->wev[g], 0));
-  }
+  };
   const long long steps = std::max(ntl - 1, 0);
+  if (use_graph && steps > 0) {
+    // The step as a CUDA graph (the groups are its parallel branches, forked
+    // from and joined to the capture stream), replayed once per time step;
+    // the step index lives in a device word that the graph's last node
+    // advances.
+    if (!h->cap_stream) CK_CUDA(h, cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+    CK_CUDA(h, h->wstep.ensure(sizeof(int)));
+    int *it_dev = h->wstep.as<int>();
+    CK_CUDA(h, cudaMemsetAsync(it_dev, 0, sizeof(int), st));
+    cudaStream_t cs = h->cap_stream;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CK_CUDA(h, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ec = cudaEventRecord(h->wev[8], cs);
+    for (int g = 0; g < G && ec == cudaSuccess; ++g) ec = cudaStreamWaitEvent(h->wst[g], h->wev[8], 0);
+    if (ec == cudaSuccess) step(0, it_dev);
+    for (int g = 0; g < G && ec == cudaSuccess; ++g) {
+      ec = cudaEventRecord(h->wev[g], h->wst[g]);
+      if (ec == cudaSuccess) ec = cudaStreamWaitEvent(cs, h->wev[g], 0);
+    }
+    if (ec == cudaSuccess) {
+      k_step_advance<<<1, 32, 0, cs>>>(it_dev);
+      ec = cudaGetLastError();
+    }
+    const cudaError_t ee = cudaStreamEndCapture(cs, &graph);
+    if (ec == cudaSuccess) ec = ee;
+    if (ec == cudaSuccess) ec = cudaGraphInstantiate(&exec, graph, 0);
+    for (long long s = 0; s < steps && ec == cudaSuccess; ++s) ec = cudaGraphLaunch(exec, st);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (ec != cudaSuccess)
+      return fail(h, EFWI_ERR_CUDA, "graph of the window time step: %s", cudaGetErrorString(ec));
+    nrec_launch *= steps;
+    h->launches[K_OTHER] += steps;
+  } else {
+    for (int it = 0; it <= ntl - 2; ++it) step(it, nullptr);
+    for (int g = 0; g < G; ++g) {
+      CK_CUDA(h, cudaEventRecord(h->wev[g], h->wst[g]));
+      CK_CUDA(h, cudaStreamWaitEvent(st, h->wev[g], 0));
+    }
+  }
   h->launches[K_STRESS_FWD] += steps * n;
   h->launches[K_VELOCITY_FWD] += steps * n;
   h->launches[K_RECORD] += nrec_launch;
@@ -1204,6 +1277,7 @@ void efwi_destroy(EfwiHandle *h) {
   for (cudaEvent_t e : h->wev)
     if (e) cudaEventDestroy(e);
   for (EfwiHandle *c : h->lane) efwi_destroy(c);
+  for (auto &w : h->wsub) efwi_destroy(w.second);
   if (h->own_st) cudaStreamDestroy(h->own_st);
   if (h->lane_fork) cudaEventDestroy(h->lane_fork);
   delete h;
@@ -1345,6 +1419,7 @@ int efwi_set_survey(EfwiHandle *h, int nshot, const EfwiShot *shots, const float
     CK_CUDA(h, h->stf.ensure(sizeof(float) * tap.size()));
     CK_CUDA(h, cudaMemcpy(h->stf.p, tap.data(), sizeof(float) * tap.size(), cudaMemcpyHostToDevice));
   }
+  h->stf_host.assign(stf, stf + (size_t)nshot * g.nt);
   h->shots.swap(out);
   h->survey_set = true;
   return EFWI_OK;
@@ -1632,17 +1707,27 @@ static int lane_sync(EfwiHandle *h, EfwiHandle *c) {
 // Allocates the large per-shot workspace of a reference-mode call up front;
 // false (with the workspace released and the error cleared) when the GPU
 // has no room for it.
-static bool lane_reserve(EfwiHandle *c, bool grad) {
+// Reference mode: state, images and the boundary-shell store; exact mode:
+// state, images, the two adjoint memory-variable sets and `ck_bytes` of
+// checkpoint slots.
+static bool lane_reserve(EfwiHandle *c, bool grad, int mode = EFWI_MODE_REFERENCE,
+                         long long ck_bytes = 0) {
   const long long N = c->N;
+  const long long P = psi_per_shot(c->geo);
   cudaError_t e = c->fields.ensure(sizeof(float) * 9 * N);
-  if (e == cudaSuccess) e = c->psi.ensure(sizeof(float) * psi_per_shot(c->geo));
+  if (e == cudaSuccess) e = c->psi.ensure(sizeof(float) * P);
   if (grad && e == cudaSuccess) e = c->adj.ensure(sizeof(float) * 9 * N);
   if (grad && e == cudaSuccess) e = c->grad.ensure(sizeof(float) * 3 * N);
-  if (grad && e == cudaSuccess)
+  if (grad && mode == EFWI_MODE_REFERENCE && e == cudaSuccess)
     e = c->shell.ensure(sizeof(float) * 9 * (size_t)std::max(c->npts, 1) * c->grid.nt);
+  if (grad && mode == EFWI_MODE_EXACT && e == cudaSuccess)
+    e = c->apsi.ensure(sizeof(float) * 2 * P);
+  if (grad && mode == EFWI_MODE_EXACT && e == cudaSuccess && ck_bytes > 0)
+    e = c->ckpt.ensure((size_t)ck_bytes);
   if (e == cudaSuccess) return true;
   cudaGetLastError();
   c->fields.release(); c->psi.release(); c->adj.release(); c->grad.release(); c->shell.release();
+  c->apsi.release(); c->ckpt.release();
   return false;
 }
 
@@ -1655,7 +1740,8 @@ static bool lane_reserve(EfwiHandle *c, bool grad) {
 // the shots in order (as with one lane); the images are the lanes'
 // accumulators added in lane order.
 static int gradient_lanes(EfwiHandle *h, int n, const int *ids, const float *obs, double *misfit,
-                          float *glam, float *gmu, float *grho, float *res_out, cudaStream_t st) {
+                          float *glam, float *gmu, float *grho, float *res_out, cudaStream_t st,
+                          int mode = EFWI_MODE_REFERENCE) {
   const bool grad = glam != nullptr;
   const int nt = h->grid.nt;
   int L = std::min(h->lanes, n);
@@ -1663,17 +1749,22 @@ static int gradient_lanes(EfwiHandle *h, int n, const int *ids, const float *obs
     int rc = get_encoder(h);  // once, before any thread needs it
     if (rc) return rc;
   }
-  if (!lane_reserve(h, grad)) L = 1;
+  // exact mode: every lane takes an equal share of the checkpoint budget
+  const long long budget = h->ck_budget;
+  auto share = [&](int lanes) { return budget / std::max(lanes, 1); };
+  if (!lane_reserve(h, grad, mode, mode == EFWI_MODE_EXACT ? share(L) : 0)) L = 1;
   while ((int)h->lane.size() < L - 1) h->lane.push_back(new EfwiHandle());
   int got = 1;
   for (; got < L; ++got) {
     EfwiHandle *c = h->lane[got - 1];
     if (lane_sync(h, c)) return fail(h, EFWI_ERR_CUDA, "lane %d: %s", got, c->err.c_str());
-    if (!lane_reserve(c, grad)) break;
+    if (!lane_reserve(c, grad, mode, mode == EFWI_MODE_EXACT ? share(L) : 0)) break;
   }
   L = got;
   if (L < 2)
-    return gradient_impl(h, n, ids, obs, EFWI_MODE_REFERENCE, misfit, glam, gmu, grho, res_out, st);
+    return gradient_impl(h, n, ids, obs, mode, misfit, glam, gmu, grho, res_out, st);
+  h->ck_budget = share(L);
+  for (int l = 1; l < L; ++l) h->lane[l - 1]->ck_budget = share(L);
   std::vector<int> b(L + 1);
   for (int l = 0; l <= L; ++l) b[l] = (int)((long long)n * l / L);
   std::vector<long long> off(n + 1, 0);
@@ -1688,6 +1779,7 @@ static int gradient_lanes(EfwiHandle *h, int n, const int *ids, const float *obs
     c->scr_syn = h->scr_syn ? h->scr_syn + o : nullptr;
     c->scr_obs = h->scr_obs ? h->scr_obs + o : nullptr;
     c->scr_res = h->scr_res ? h->scr_res + o : nullptr;
+    c->gstf = h->gstf ? h->gstf + (size_t)b[l] * nt : nullptr;
     CK_CUDA(h, cudaStreamWaitEvent(c->own_st, h->lane_fork, 0));
   }
   // No return between the first thread's start and the joins below.
@@ -1702,9 +1794,9 @@ static int gradient_lanes(EfwiHandle *h, int n, const int *ids, const float *obs
       rcs[l] = fail(c, EFWI_ERR_CUDA, "cudaSetDevice(%d) failed in lane %d", dev, l);
       return;
     }
-    rcs[l] = gradient_impl(c, b[l + 1] - b[l], ids + b[l], obs + o, EFWI_MODE_REFERENCE, nullptr,
-                           glam, gmu, grho, res_out ? res_out + o : nullptr, c->own_st, false,
-                           false, js.data() + b[l]);
+    rcs[l] = gradient_impl(c, b[l + 1] - b[l], ids + b[l], obs + o, mode, nullptr, glam, gmu,
+                           grho, res_out ? res_out + o : nullptr, c->own_st, false, false,
+                           js.data() + b[l]);
   };
   for (int l = 1; l < L; ++l) {
     try {
@@ -1713,9 +1805,14 @@ static int gradient_lanes(EfwiHandle *h, int n, const int *ids, const float *obs
       run_lane(l);  // no thread to spare: the lane runs here, before lane 0
     }
   }
-  rcs[0] = gradient_impl(h, b[1], ids, obs, EFWI_MODE_REFERENCE, nullptr, glam, gmu, grho, res_out,
-                         st, false, false, js.data());
+  rcs[0] = gradient_impl(h, b[1], ids, obs, mode, nullptr, glam, gmu, grho, res_out, st, false,
+                         false, js.data());
   for (std::thread &t : th) t.join();
+  h->ck_budget = budget;
+  for (int l = 1; l < L; ++l) {
+    EfwiHandle *c = h->lane[l - 1];
+    h->ck_forward_steps = std::max(h->ck_forward_steps, c->ck_forward_steps);
+  }
   for (int l = 1; l < L; ++l) {
     EfwiHandle *c = h->lane[l - 1];
     if (h->prof_sample > 0) resolve_profile(c);
@@ -1775,8 +1872,8 @@ int efwi_gradient(EfwiHandle *h, int n, const int *ids, const float *obs, int mo
   if (!glam || !gmu || !grho) return fail(h, EFWI_ERR_ARG, "null gradient output");
   if (mode != EFWI_MODE_REFERENCE && mode != EFWI_MODE_EXACT)
     return fail(h, EFWI_ERR_ARG, "gradient mode %d is not available", mode);
-  if (mode == EFWI_MODE_REFERENCE && h->lanes > 1 && n > 1)
-    return gradient_lanes(h, n, ids, obs, misfit, glam, gmu, grho, res, (cudaStream_t)stream);
+  if (h->lanes > 1 && n > 1)
+    return gradient_lanes(h, n, ids, obs, misfit, glam, gmu, grho, res, (cudaStream_t)stream, mode);
   return gradient_impl(h, n, ids, obs, mode, misfit, glam, gmu, grho, res, (cudaStream_t)stream);
 }
 
@@ -1894,7 +1991,8 @@ int efwi_forward_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow 
   float *ttm = h->traces_tm.as<float>();
   if (h->variant == 1) {
     long long *dsrc = (long long *)((char *)drr + b_rec);
-    rc = window_loop_tma(h, dom, rec_dom, ddom, drd, drc, drr, dsrc, ttm, ntl, st);
+    rc = window_loop_tma(h, dom, rec_dom, ddom, drd, drc, drr, dsrc, ttm, ntl,
+                         use_graph && h->prof_sample == 0, st);
     if (rc) return rc;
     return window_traces(h, dom, traces, st);
   }
@@ -1934,6 +2032,127 @@ int efwi_forward_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow 
   h->launches[K_VELOCITY_FWD] += ntl - 1;
   if (nr > 0) h->launches[K_RECORD] += ntl - 1;
   return window_traces(h, dom, traces, st);
+}
+
+int efwi_gradient_windows(EfwiHandle *h, int n, const int *ids, const EfwiWindow *win,
+                          const float *obs, int mode, double *misfit, float *g_lam, float *g_mu,
+                          float *g_rho, void *stream) {
+  int rc = check_ready(h, n, ids);
+  if (rc) return rc;
+  if (n > 0 && (!win || !obs)) return fail(h, EFWI_ERR_ARG, "null windows or observed data");
+  if (!g_lam || !g_mu || !g_rho) return fail(h, EFWI_ERR_ARG, "null gradient output");
+  if (mode != EFWI_MODE_REFERENCE && mode != EFWI_MODE_EXACT)
+    return fail(h, EFWI_ERR_ARG, "gradient mode %d is not available", mode);
+  cudaStream_t st = (cudaStream_t)stream;
+  const EfwiGrid &G = h->grid;
+  const int np = G.npml, nt = G.nt;
+  const long long ncell = (long long)G.nz * G.nx * G.ny;
+  for (float *g : {g_lam, g_mu, g_rho}) CK_CUDA(h, cudaMemsetAsync(g, 0, sizeof(float) * ncell, st));
+  double J = 0.0;
+  long long obs_off = 0;
+  for (int k = 0; k < n; ++k) {
+    const EfwiWindow &w = win[k];
+    const ShotHost &sh = h->shots[ids[k]];
+    const long long ntr = 3LL * sh.nrec * nt;
+    if (w.nx < 2 * np + 5 || w.ny < 2 * np + 5 || w.x0 < 0 || w.y0 < 0 || w.x0 + w.nx > G.nx ||
+        w.y0 + w.ny > G.ny)
+      return fail(h, EFWI_ERR_ARG, "window %d (%d+%d, %d+%d) invalid for grid %d x %d, npml %d", k,
+                  w.x0, w.nx, w.y0, w.ny, G.nx, G.ny, np);
+    // the window's engine: its own grid and C-PML, the handle's tuning
+    EfwiHandle *&W = h->wsub[{w.nx, w.ny}];
+    if (!W) {
+      EfwiGrid gw = G;
+      gw.nx = w.nx;
+      gw.ny = w.ny;
+      rc = efwi_create(&gw, &W);
+      if (rc) {
+        const std::string e = W ? W->err : std::string("efwi_create failed");
+        efwi_destroy(W);
+        W = nullptr;
+        return fail(h, rc, "window %d: %s", k, e.c_str());
+      }
+    }
+    W->if_win = h->if_win; W->bx = h->bx; W->zchunk = h->zchunk; W->max_batch = 1;
+    W->variant = h->variant; W->fcfg = h->fcfg; W->rcfg = h->rcfg; W->zchunk_rev = h->zchunk_rev;
+    W->nt_limit = h->nt_limit; W->use_graphs = h->use_graphs; W->ck_budget = h->ck_budget;
+    W->lanes = 1;
+    // model: the window of the resident model volumes (as efwi_forward_windows)
+    CK_CUDA(W, W->lam.ensure(sizeof(float) * W->N));
+    CK_CUDA(W, W->mu.ensure(sizeof(float) * W->N));
+    CK_CUDA(W, W->buoy.ensure(sizeof(float) * W->N));
+    const float *src[3] = {h->lam.as<float>(), h->mu.as<float>(), h->buoy.as<float>()};
+    float *dst[3] = {W->lam.as<float>(), W->mu.as<float>(), W->buoy.as<float>()};
+    for (int v = 0; v < 3; ++v)
+      k_window_slice<<<592, 256, 0, st>>>(src[v], dst[v], G.nz, G.nx, h->py, w.x0, w.y0, w.nx,
+                                          w.ny, W->py);
+    h->launches[K_OTHER] += 3;
+    W->model_set = true;
+    // survey: the shot with window-relative coordinates and the receivers
+    // inside the window
+    const long long sc = sh.src_cell;
+    const int sy = (int)(sc % h->py), sx = (int)((sc / h->py) % G.nx), sz = (int)(sc / h->py / G.nx);
+    std::vector<int> zr, xr, yr, sel;
+    for (int r = 0; r < sh.nrec; ++r) {
+      const long long c = sh.rec_cell[r];
+      const int y = (int)(c % h->py), x = (int)((c / h->py) % G.nx), z = (int)(c / h->py / G.nx);
+      if (x < w.x0 || x >= w.x0 + w.nx || y < w.y0 || y >= w.y0 + w.ny) continue;
+      zr.push_back(z); xr.push_back(x - w.x0); yr.push_back(y - w.y0); sel.push_back(r);
+    }
+    std::vector<float> w0, w1, wt;
+    for (int r : sel) { w0.push_back(sh.win0[r]); w1.push_back(sh.win1[r]); wt.push_back(sh.wts[r]); }
+    EfwiShot es{};
+    es.z_src = sz; es.x_src = sx - w.x0; es.y_src = sy - w.y0;
+    es.nrec = (int)sel.size();
+    es.z_rec = zr.data(); es.x_rec = xr.data(); es.y_rec = yr.data();
+    es.win_start = w0.data(); es.win_end = w1.data(); es.weights = wt.data();
+    es.src_weight = sh.src_w;
+    rc = efwi_set_survey(W, 1, &es, h->stf_host.data() + (size_t)ids[k] * nt);
+    if (rc) return fail(h, rc, "window %d: %s", k, W->err.c_str());
+    // observed data of those receivers
+    const long long nw = 3LL * (long long)sel.size() * nt;
+    CK_CUDA(h, h->wobs.ensure(sizeof(float) * std::max(nw, 1LL)));
+    if (!sel.empty()) {
+      CK_CUDA(h, h->wsel.ensure(sizeof(int) * sel.size()));
+      CK_CUDA(h, cudaMemcpyAsync(h->wsel.p, sel.data(), sizeof(int) * sel.size(),
+                                 cudaMemcpyHostToDevice, st));
+      k_gather_rows<<<592, 256, 0, st>>>(obs + obs_off, h->wsel.as<int>(), (int)sel.size(),
+                                         sh.nrec, nt, h->wobs.as<float>());
+      h->launches[K_OTHER]++;
+    }
+    const long long nwc = (long long)G.nz * w.nx * w.ny;
+    CK_CUDA(h, h->wimg.ensure(sizeof(float) * 3 * nwc));
+    float *gw = h->wimg.as<float>();
+    const int zero = 0;
+    double Jk = 0.0;
+    rc = efwi_gradient(W, 1, &zero, h->wobs.as<float>(), mode, &Jk, gw, gw + nwc, gw + 2 * nwc,
+                       nullptr, st);
+    if (rc) return fail(h, rc, "window %d: %s", k, W->err.c_str());
+    float *outs[3] = {g_lam, g_mu, g_rho};
+    for (int v = 0; v < 3; ++v)
+      k_window_add<<<592, 256, 0, st>>>(outs[v], gw + v * nwc, G.nz, G.nx, G.ny, w.x0, w.y0, w.nx,
+                                        w.ny);
+    h->launches[K_OTHER] += 3;
+    // One window's workspace at a time: the window engine keeps its grid,
+    // coefficients and shell table, and gives back its state, shell store
+    // and checkpoints (their graphs go with them).
+    CK_CUDA(h, cudaStreamSynchronize(st));
+    for (DevBuf *b : {&W->fields, &W->psi, &W->adj, &W->grad, &W->shell, &W->ckpt, &W->apsi,
+                      &W->traces_tm, &W->res_tm})
+      b->release();
+    W->g_fwd.reset();
+    W->g_rev.reset();
+    for (int c = 0; c < K_NCLASS; ++c) {
+      h->launches[c] += W->launches[c];
+      W->launches[c] = 0;
+    }
+    J += Jk;
+    obs_off += ntr;
+  }
+  rc = check_launch(h, "window gradients");
+  if (rc) return rc;
+  CK_CUDA(h, cudaStreamSynchronize(st));
+  if (misfit) *misfit = J;
+  return EFWI_OK;
 }
 
 int efwi_adjoint(EfwiHandle *h, int n, const int *ids, const float *adj_src, float *g_lam,

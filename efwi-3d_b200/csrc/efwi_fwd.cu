@@ -304,9 +304,10 @@ k_velocity_fwd_multi(const Domain *__restrict__ dom, int ndom, int ntiles, int z
 // stay zero).
 __global__ void k_record_multi(const Domain *__restrict__ dom, const int *__restrict__ rec_dom,
                                const int *__restrict__ rec_cell, const int *__restrict__ rec_r,
-                               int nrec, float *traces_tm, int it) {
+                               int nrec, float *traces_tm, int it, const int *it_dev) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nrec) return;
+  if (it_dev) it = *it_dev + 1;
   const Domain &d = dom[rec_dom[u]];
   const int i = rec_cell[u], r = rec_r[u];
   float *t = traces_tm + d.trace_off + (long long)it * 3 * d.nrec;

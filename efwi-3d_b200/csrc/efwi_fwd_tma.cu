@@ -70,7 +70,8 @@ k_stress_fwd_tma(const __grid_constant__ Maps<11> maps, Geo g, Fields f, Psi ps,
     Kyh = g.cy[CKH * ny + y]; ayh = g.cy[CAH * ny + y]; byh = g.cy[CBH * ny + y];
   }
   const long long src_cell = src.cell ? src.cell[shot] : -1;
-  const float src_amp = src.stf ? src.stf[(long long)shot * src.nt + src.it] : 0.f;
+  const int sit = src.it_dev ? *src.it_dev : src.it;
+  const float src_amp = src.stf ? src.stf[(long long)shot * src.nt + sit] : 0.f;
 
   int i = act ? (int)cell(g, z0, x, y) : 0;
   float qz0 = 0.f, qz1 = 0.f, qz2 = 0.f, qz3 = 0.f, qx0 = 0.f, qx1 = 0.f, qx2 = 0.f, qx3 = 0.f;

@@ -13,6 +13,9 @@ struct SrcArgs {
   const float *stf;
   int nt;
   int it;
+  // when set, the step index is read from this device word instead of `it`
+  // (a launch replayed from a CUDA graph step after step)
+  const int *it_dev;
 };
 
 // Receivers of the shots of one launch, grouped by cell so that several
@@ -84,8 +87,11 @@ struct Domain {
 int multi_blocks(int bx);
 void launch_fwd_multi(int bx, int blocks, cudaStream_t st, const Domain *dom, int ndom, int ntiles,
                       int zchunk, int it);
+// Receivers of windowed shots at sample `it`, or at 1 + *it_dev when it_dev
+// is set.
 __global__ void k_record_multi(const Domain *dom, const int *rec_dom, const int *rec_cell,
-                               const int *rec_r, int nrec, float *traces_tm, int it);
+                               const int *rec_r, int nrec, float *traces_tm, int it,
+                               const int *it_dev = nullptr);
 
 // Host launchers of the stencil kernels (bx: x rows per CTA, 4 or 8; the
 // CTA is 32 x bx threads).

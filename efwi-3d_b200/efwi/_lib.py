@@ -83,6 +83,9 @@ _SIGS = {
                                       C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_forward_windows": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
                                        C.c_void_p, C.c_int, C.c_void_p]),
+    "efwi_gradient_windows": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
+                                        C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_void_p]),
     "efwi_illumination": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,

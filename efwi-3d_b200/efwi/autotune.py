@@ -51,7 +51,7 @@ def _time_call(P, ids, obs, reps: int = 2) -> float:
 def autotune(P, shot_id: int, obs_shot: torch.Tensor, nt_probe: int = 16,
              fwd_cfgs: Sequence[int] = FWD_CFGS, rev_cfgs: Sequence[int] = REV_CFGS,
              zchunks: Sequence[int] = ZCHUNKS, pair_ids=None, pair_obs=None,
-             lanes_nt: int = 64) -> Dict:
+             lanes_nt: int = 160, lanes_reps: int = 3) -> Dict:
     """Tunes `P` (a Propagator with model and survey set) on shot `shot_id`
     whose observed traces are `obs_shot`; returns the timings and the choice.
 
@@ -59,7 +59,9 @@ def autotune(P, shot_id: int, obs_shot: torch.Tensor, nt_probe: int = 16,
     one lane on P, a last stage times whole two-shot calls, whose lanes
     share the GPU, for the chosen z planes per CTA and 8 (forward and
     reverse): concurrent lanes fill each other's tail waves, which favours
-    longer z marches than the kernels timed alone do."""
+    longer z marches than the kernels timed alone do.  Those candidates
+    differ by a few per cent, so each is timed `lanes_reps` times over
+    `lanes_nt` steps and its fastest run counts."""
     ids = [int(shot_id)]
     P.set_nt_limit(nt_probe)
     try:
@@ -87,7 +89,7 @@ def autotune(P, shot_id: int, obs_shot: torch.Tensor, nt_probe: int = 16,
             for cand in sorted({(zf, zr), (8, zr), (zf, 8), (8, 8)}):
                 P.set_tuning(bf[0], cand[0], br[0], cand[1])
                 _time_call(P, pair_ids, pair_obs, reps=1)  # warm
-                pair[cand] = _time_call(P, pair_ids, pair_obs)
+                pair[cand] = _time_call(P, pair_ids, pair_obs, reps=lanes_reps)
         finally:
             P.set_nt_limit(0)
         zf, zr = min(pair, key=pair.get)

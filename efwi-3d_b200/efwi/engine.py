@@ -299,6 +299,32 @@ class Propagator:
         check(self._h, rc)
         return out
 
+    def gradient_windows(self, shot_ids, windows, obs: torch.Tensor, mode: str = "reference"):
+        """Misfit and lambda/mu/rho gradients of shots each on its own window
+        (x0, y0, nx, ny) of the padded grid (efwi_gradient_windows): the
+        receivers inside a window take part, the images are added into the
+        full grid at the window's place."""
+        ids = self._ids(shot_ids)
+        if len(windows) != len(ids):
+            raise ValueError("one window per shot")
+        obs = _f32_dev(obs, self.device)
+        if obs.numel() != sum(self.trace_sizes(ids)):
+            raise ValueError("observed data size does not match the shots")
+        arr = (_lib.EfwiWindow * max(len(ids), 1))()
+        for k, w in enumerate(windows):
+            arr[k].x0, arr[k].y0, arr[k].nx, arr[k].ny = (int(v) for v in w)
+        m = {"reference": _lib.MODE_REFERENCE, "exact": _lib.MODE_EXACT}[mode]
+        gl, gm, gr = (torch.empty(self.grid.shape, device=self.device, dtype=torch.float32)
+                      for _ in range(3))
+        J = C.c_double(0.0)
+        with torch.cuda.device(self.device):
+            rc = self._L.efwi_gradient_windows(
+                self._h, len(ids), ids.ctypes.data_as(C.POINTER(C.c_int)), C.cast(arr, C.c_void_p),
+                C.c_void_p(obs.data_ptr()), m, C.byref(J), C.c_void_p(gl.data_ptr()),
+                C.c_void_p(gm.data_ptr()), C.c_void_p(gr.data_ptr()), self._stream())
+        check(self._h, rc)
+        return J.value, gl, gm, gr
+
     def adjoint(self, shot_ids, adj_src: torch.Tensor):
         """J^T adj_src: exact adjoint images (lambda, mu, rho) of the shots
         for an adjoint source in the traces layout."""

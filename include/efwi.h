@@ -156,7 +156,10 @@ int efwi_gradient(EfwiHandle *h, int n, const int *shot_ids, const float *obs, i
  * streams; use_graph is ignored.  With the L1 variant all windows of a
  * call advance together in one persistent launch per half-step (tile_bx
  * and zchunk of efwi_set_options); use_graph = 1 captures the whole time
- * loop in a CUDA graph and launches it once.  Both give the same bits.
+ * loop in a CUDA graph and launches it once.  With the TMA variant,
+ * use_graph = 1 captures one time step (every group, as parallel branches)
+ * in a CUDA graph and replays it once per step, the step index read from a
+ * device word.  All forms give the same bits.
  * traces: device, concatenation over shot_ids of [3][nrec][nt].  The call
  * synchronises the stream. */
 typedef struct {
@@ -164,6 +167,18 @@ typedef struct {
 } EfwiWindow;
 int efwi_forward_windows(EfwiHandle *h, int n, const int *shot_ids, const EfwiWindow *windows,
                          float *traces, int use_graph, void *stream);
+
+/* Misfit and gradients of shots on windows (no reference counterpart): shot
+ * k on window k as in efwi_forward_windows (its own grid and C-PML, the
+ * window of the resident model), by the gradient `mode` of efwi_gradient on
+ * that grid; the receivers inside the window take part (obs: device, the
+ * shots' full [3][nrec][nt] blocks), the images are added into the full
+ * grid's g_lam, g_mu, g_rho (device, [nz][nx][ny], zeroed here) at the
+ * window's place, and misfit is the sum over the windows.  Synchronises the
+ * stream. */
+int efwi_gradient_windows(EfwiHandle *h, int n, const int *shot_ids, const EfwiWindow *windows,
+                          const float *obs, int mode, double *misfit, float *g_lam, float *g_mu,
+                          float *g_rho, void *stream);
 
 /* J^T applied to an adjoint source (no reference counterpart): the exact
  * adjoint of the forward modelling of the shots, with the device traces

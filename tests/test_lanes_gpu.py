@@ -118,3 +118,34 @@ def test_graph_replay_matches_eager_launches():
             assert got[0] == ref[0]
             for x, y in zip(got[1:], ref[1:]):
                 assert torch.equal(x, y)
+
+
+def test_exact_mode_lanes_match_one_lane():
+    """Exact gradients on 1, 2 and 3 lanes, each lane with an equal share of
+    the checkpoint budget: the same misfit bits and residuals, images equal
+    up to the order of the per-shot sums (1e-6 rel-L2), and the source-time
+    function gradients of every shot bit for bit."""
+    from efwi.engine import Propagator
+    g, shots, stf, true, init = _problem()
+    ids = [0, 1, 2, 3, 4]
+    P = Propagator(g)
+    P.set_survey(shots, stf)
+    P.set_model(*[torch.from_numpy(m) for m in true])
+    obs = P.forward(ids)
+    P.set_model(*[torch.from_numpy(m) for m in init])
+    P.set_checkpoint_budget(24 * P.state_bytes())
+    out = {}
+    for L in (1, 2, 3):
+        P.set_lanes(L)
+        J, gl, gm, gr, gs = P.stf_gradient(ids, obs)
+        res = P.gradient(ids, obs, mode="exact", want_residual=True)[4]
+        out[L] = (J, [x.cpu() for x in (gl, gm, gr)], gs.cpu(), res.cpu())
+    J1, g1, s1, r1 = out[1]
+    for L in (2, 3):
+        J, gg, ss, rr = out[L]
+        assert J == J1
+        assert torch.equal(rr, r1)
+        assert torch.equal(ss, s1)
+        for a, b in zip(gg, g1):
+            d = float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+            assert d < 1e-6

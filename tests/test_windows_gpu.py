@@ -126,3 +126,46 @@ def test_tma_windows_on_eight_streams_equal_the_multi_domain_launch():
     out = P.forward_windows(ids, wins).cpu()
     assert float(ref.abs().max()) > 0
     assert torch.equal(out, ref)
+
+
+@pytest.mark.parametrize("mode", ["reference", "exact"])
+def test_window_gradients_match_each_window_alone(mode):
+    """efwi_gradient_windows against each window's problem run alone (its
+    own grid, the window of the model, the receivers inside it): the misfit
+    is the sum of the windows' misfits and the images are the windows'
+    images added at their places, bit for bit."""
+    from efwi.engine import Grid, Propagator, Shot
+    g, shots, stf, model, windows = _problem()
+    ids = [0, 1, 2]
+    true = [m * np.float32(1.03) for m in model]
+    P = Propagator(g)
+    P.set_survey(shots, stf)
+    P.set_model(*[torch.from_numpy(m) for m in true])
+    obs = P.forward(ids)
+    P.set_model(*[torch.from_numpy(m) for m in model])
+    J, gl, gm, gr = P.gradient_windows(ids, windows, obs, mode=mode)
+    parts = P.split(obs, ids)
+    Jsum = 0.0
+    acc = [np.zeros(g.shape, np.float32) for _ in range(3)]
+    for k, (shot, w) in enumerate(zip(shots, windows)):
+        x0, y0, nxw, nyw = w
+        gw = Grid(g.nz, nxw, nyw, g.npml, g.nt, g.dz, g.dx, g.dy, g.dt, g.f0)
+        inside = ((shot.x_rec >= x0) & (shot.x_rec < x0 + nxw) & (shot.y_rec >= y0) &
+                  (shot.y_rec < y0 + nyw))
+        sw = Shot(src=(shot.src[0], shot.src[1] - x0, shot.src[2] - y0),
+                  z_rec=shot.z_rec[inside], x_rec=(shot.x_rec[inside] - x0).astype(np.int32),
+                  y_rec=(shot.y_rec[inside] - y0).astype(np.int32))
+        Q = Propagator(gw)
+        Q.set_lanes(1)
+        Q.set_survey([sw], stf[k][None, :])
+        Q.set_model(*[torch.from_numpy(np.ascontiguousarray(m[:, x0:x0 + nxw, y0:y0 + nyw]))
+                      for m in model])
+        ob = parts[k].view(3, shot.nrec, g.nt)[:, torch.from_numpy(inside).to(obs.device)]
+        Jk, *gk = Q.gradient([0], ob.contiguous().reshape(-1), mode=mode)
+        Jsum += Jk
+        for a, b in zip(acc, gk):
+            a[:, x0:x0 + nxw, y0:y0 + nyw] += b.cpu().numpy()
+        Q.close()
+    assert J == Jsum
+    for a, b in zip((gl, gm, gr), acc):
+        assert np.array_equal(a.cpu().numpy(), b)
