@@ -537,11 +537,38 @@ def run_cnn(a):
     (the input gradient and the weight gradient add two more convolutions
     per layer in the backward pass)."""
     import torch
-    from efwi.cnn import Preconditioner
+    from efwi.cnn import Preconditioner, conv3d_raw, conv3d_status, set_conv_kernel
     torch.cuda.set_device(0)
+    vox = a.n ** 3
+    fl1 = 2.0 * 27 * 16 * 16 * vox            # one layer
+    by1 = 2 * 16 * 2 * vox                    # bf16 in + bf16 out
+    d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = float(d.get("bf16_tflops", 1590.0))
+    hbm = float(d.get("hbm_gbs", 6650.0))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(a.n, a.n, a.n, 16, device="cuda", generator=g).to(torch.bfloat16)
+    w = (0.2 * torch.randn(27, 16, 16, device="cuda", generator=g)).to(torch.bfloat16)
+    forms = {}
+    for form in ("mma", "tcgen05"):
+        set_conv_kernel(form)
+        for _ in range(3):
+            conv3d_raw(x, w, None, True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            conv3d_raw(x, w, None, True)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        forms[form] = {"layer_ms": ms, "tflops": fl1 / (ms * 1e-3) / 1e12,
+                       "frac_bf16": fl1 / (ms * 1e-3) / 1e12 / peak,
+                       "gbs": by1 / (ms * 1e-3) / 1e9, "frac_hbm": by1 / (ms * 1e-3) / 1e9 / hbm}
+    if conv3d_status():
+        raise RuntimeError("a tcgen05 convolution timed out waiting for its tensor cores")
+    set_conv_kernel("tcgen05")
     net = Preconditioner(cin=3, seed=0).cuda()
     feats = torch.randn(3, a.n, a.n, a.n, device="cuda")
-    vox = a.n ** 3
     layers = len(net.w)
     for _ in range(3):
         net(feats).sum().backward()
@@ -559,15 +586,14 @@ def run_cnn(a):
     torch.cuda.synchronize()
     fwd_ms = e[0].elapsed_time(e[1]) / a.steps
     all_ms = e[2].elapsed_time(e[3]) / a.steps
-    fl = 2.0 * 27 * 16 * 16 * vox * layers
-    d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
-        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    peak = float(d.get("bf16_tflops", 1590.0))
+    fl = fl1 * layers
     print(json.dumps({"case": "cnn", "grid": a.n, "layers": layers, "fwd_ms": fwd_ms,
                       "fwd_bwd_ms": all_ms, "fwd_tflops": fl / (fwd_ms * 1e-3) / 1e12,
                       "fwd_bwd_tflops": 3 * fl / (all_ms * 1e-3) / 1e12,
-                      "peak_bf16_tflops": peak,
-                      "note": "mma.sync m16n8k16 BF16 kernels, FP32 accumulation"}))
+                      "one_layer_bf16_relu": forms,
+                      "peak_bf16_tflops": peak, "peak_hbm_gbs": hbm,
+                      "note": "network: tcgen05 forward and input-gradient convolutions, "
+                              "mma.sync weight gradient; FP32 accumulation"}))
 
 
 def main():

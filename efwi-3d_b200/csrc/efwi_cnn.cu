@@ -24,6 +24,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <atomic>
+
+#include "efwi_tma.cuh"
+
 namespace efwi {
 namespace {
 
@@ -195,17 +200,234 @@ __global__ void k_reduce_partials(const float *__restrict__ partial, int nparts,
   out[i] = s;
 }
 
+
+// ------------------------------------------------------------- tcgen05 form
+// The forward convolution on the 5th-generation tensor cores: per tile of
+// 128 voxels (8 x by 16 y at one z) and tap t, D[128 voxels][16 co] +=
+// A_t[128][16 ci] B_t[16 ci][16 co] with one tcgen05.mma.kind::f16 (M 128,
+// N 16, K 16; BF16 operands from shared memory, FP32 accumulator in TMEM).
+// The CTA's input tile with its 1-voxel halo (3 x 18 x 10 voxels) is staged
+// as two planes of 16-byte chunks (channels 0-7, channels 8-15), x fastest,
+// so that A_t is the canonical K-major, non-swizzled operand at a shifted
+// base: core matrices of 8 rows (8 consecutive x) x 16 bytes, the 16 rows
+// of the tile one staged row apart (SBO = 10 x 16 B), the two K halves one
+// plane apart (LBO).  B_t is staged the same way ([t][half][co][8 ci]).  One
+// thread issues the 27 MMAs and commits them to an mbarrier; each warp then
+// reads its 32 TMEM lanes (32 voxels x 16 fp32 columns) with tcgen05.ld.
+// CTAs are persistent (the weights are staged once per CTA) and hold 32 TMEM
+// columns each, allocated on entry and freed on exit.
+constexpr int kTcX = 8, kTcY = 16;                   // tile: 128 voxels
+constexpr int kTcSX = kTcX + 2, kTcSY = kTcY + 2;    // staged with the halo
+constexpr int kTcVox = 3 * kTcSY * kTcSX;            // 540 staged voxels
+constexpr int kTcPlane = kTcVox * 16;                // bytes of one channel-half plane
+constexpr int kTcWBytes = 27 * 2 * kC * 16;          // staged weights
+constexpr int kTcSmem = 2 * kTcPlane + kTcWBytes;
+
+// Shared-memory matrix descriptor of tcgen05.mma: start address, leading
+// (K) and stride (M/N) byte offsets, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N = 16, M = 128.
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) |
+                              ((128u >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(kTcIdesc), "r"(acc));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ int g_conv_status;  // EFWI_STATUS_TIMEOUT after a wait that ran out
+
+__global__ void __launch_bounds__(128)
+k_conv3d_fwd_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
+                const float *__restrict__ bias, int D, int H, int W, int relu,
+                __nv_bfloat16 *__restrict__ yb, float *__restrict__ yf) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  unsigned char *sx = smem;                     // [half][z][y][x] x 16 B
+  unsigned char *swt = smem + 2 * kTcPlane;     // [t][half][co] x 16 B
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int k = tid; k < 27 * 2 * kC; k += blockDim.x) {
+    const int t = k / (2 * kC), r = k % (2 * kC), h = r / kC, co = r % kC;
+    *reinterpret_cast<uint4 *>(swt + ((t * 2 + h) * kC + co) * 16) =
+        *reinterpret_cast<const uint4 *>(w + (t * kC + co) * kC + h * 8);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(
+                     smem_u32(&tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t sxa = smem_u32(sx), swa = smem_u32(swt);
+  const int ntx = (W + kTcX - 1) / kTcX, nty = (H + kTcY - 1) / kTcY;
+  const long long ntiles = (long long)ntx * nty * D;
+  int phase = 0;
+  bool ok = true;
+  for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int tx = (int)(tile % ntx);
+    const long long r = tile / ntx;
+    const int ty = (int)(r % nty), z = (int)(r / nty);
+    const int x0 = tx * kTcX, y0 = ty * kTcY;
+    for (int c = tid; c < 2 * kTcVox; c += blockDim.x) {
+      const int v = c >> 1, h = c & 1;
+      const int xx = v % kTcSX, t2 = v / kTcSX;
+      const int yy = t2 % kTcSY, zz = t2 / kTcSY;
+      const int gz = z - 1 + zz, gy = y0 - 1 + yy, gx = x0 - 1 + xx;
+      uint4 val = make_uint4(0u, 0u, 0u, 0u);
+      if (gz >= 0 && gz < D && gy >= 0 && gy < H && gx >= 0 && gx < W)
+        val = *reinterpret_cast<const uint4 *>(x + (((long long)gz * H + gy) * W + gx) * kC + h * 8);
+      *reinterpret_cast<uint4 *>(sx + h * kTcPlane + v * 16) = val;
+    }
+    // the staged tile (generic-proxy writes) is read by the tensor cores
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+      for (int t = 0; t < 27; ++t) {
+        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+        const uint32_t a = sxa + (uint32_t)(((dz * kTcSY + dy) * kTcSX + dx) * 16);
+        const uint64_t ad = tc_desc(a, kTcPlane, kTcSX * 16);
+        const uint64_t bd = tc_desc(swa + (uint32_t)(t * 2 * kC * 16), kC * 16, 8 * 16);
+        tc_mma(tmem, ad, bd, t > 0 ? 1u : 0u);
+      }
+      tc_commit(&bar);
+    }
+    // every thread decides on the same value: tcgen05.ld is warp-collective
+    const bool got = __syncthreads_and(mbar_wait_bounded(&bar, (uint32_t)phase));
+    phase ^= 1;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (got) {
+      float v[16];
+      tc_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
+      const int m = warp * 32 + lane;
+      const int xv = x0 + (m & 7), yv = y0 + (m >> 3);
+      if (xv < W && yv < H) {
+        const long long off = (((long long)z * H + yv) * W + xv) * kC;
+        float o[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          o[k] = v[k] + (bias ? bias[k] : 0.f);
+          if (relu) o[k] = fmaxf(o[k], 0.f);
+        }
+        if (yb) {
+          uint32_t pk[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(o[2 * k], o[2 * k + 1]);
+            pk[k] = *reinterpret_cast<const uint32_t *>(&b2);
+          }
+          uint4 *dst = reinterpret_cast<uint4 *>(yb + off);
+          dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        }
+        if (yf) {
+          float4 *dst = reinterpret_cast<float4 *>(yf + off);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) dst[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // TMEM and the staged tile are free again
+    ok = got;
+  }
+  if (!ok && tid == 0) {
+    atomicExch(&g_conv_status, EFWI_STATUS_TIMEOUT);
+    mbar_wait_bounded(&bar, (uint32_t)(phase ^ 1));  // the MMAs still in flight, bounded
+  }
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+}
+
 }  // namespace
 }  // namespace efwi
 
 using namespace efwi;
 
+namespace {
+std::atomic<int> g_conv_kernel{0};  // 1: tcgen05 form, 0: mma.sync form
+std::atomic<unsigned long long> g_tc_smem_set{0};
+int g_sm_count[64] = {0};
+}  // namespace
+
+extern "C" int efwi_conv3d_set_kernel(int tcgen05) {
+  g_conv_kernel.store(tcgen05 ? 1 : 0);
+  return 0;
+}
+
+extern "C" int efwi_conv3d_status(int *timed_out, void *stream) {
+  if (!timed_out) return 1;
+  int v = 0, zero = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyFromSymbolAsync(&v, g_conv_status, sizeof(int), 0, cudaMemcpyDeviceToHost, st) !=
+          cudaSuccess ||
+      cudaMemcpyToSymbolAsync(g_conv_status, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return 2;
+  *timed_out = v != 0;
+  return 0;
+}
+
 extern "C" int efwi_conv3d_forward(const void *x, const void *w, const float *bias, int D, int H,
                                    int W, int relu, void *y_bf16, float *y_f32, void *stream) {
   if (!x || !w || D < 1 || H < 1 || W < 1 || D > 65535 || (!y_bf16 && !y_f32)) return 1;
   if (((uintptr_t)x & 15) != 0) return 1;  // staged with 16-byte loads
+  cudaStream_t st = (cudaStream_t)stream;
+  if (g_conv_kernel.load() == 1 && ((uintptr_t)w & 15) == 0 && ((uintptr_t)y_bf16 & 15) == 0 &&
+      ((uintptr_t)y_f32 & 15) == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 2;
+    int &sms = g_sm_count[dev & 63];
+    if (!sms && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return 2;
+    set_smem_once(k_conv3d_fwd_tc, kTcSmem, g_tc_smem_set);
+    const long long tiles = (long long)((W + kTcX - 1) / kTcX) * ((H + kTcY - 1) / kTcY) * D;
+    const int blocks = (int)std::min<long long>(tiles, 6LL * sms);
+    k_conv3d_fwd_tc<<<blocks, 128, kTcSmem, st>>>((const __nv_bfloat16 *)x,
+                                                  (const __nv_bfloat16 *)w, bias, D, H, W, relu,
+                                                  (__nv_bfloat16 *)y_bf16, y_f32);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+  }
   const dim3 grid((W + kTileX - 1) / kTileX, (H + kRowsFwd - 1) / kRowsFwd, D);
-  k_conv3d_fwd<<<grid, 32 * kRowsFwd, 0, (cudaStream_t)stream>>>(
+  k_conv3d_fwd<<<grid, 32 * kRowsFwd, 0, st>>>(
       (const __nv_bfloat16 *)x, (const __nv_bfloat16 *)w, bias, D, H, W, relu,
       (__nv_bfloat16 *)y_bf16, y_f32);
   return cudaGetLastError() == cudaSuccess ? 0 : 2;

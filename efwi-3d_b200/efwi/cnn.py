@@ -43,6 +43,27 @@ def conv3d_raw(x: torch.Tensor, wb: torch.Tensor, bias, relu: bool, out_f32: boo
     return yf if out_f32 else yb
 
 
+def set_conv_kernel(form: str) -> None:
+    """'tcgen05' (tensor-memory accumulator, one MMA per tap for 128 voxels)
+    or 'mma' (mma.sync m16n8k16) for every later forward / input-gradient
+    convolution of this process."""
+    if form not in ("tcgen05", "mma"):
+        raise ValueError(f"unknown convolution kernel form {form!r}")
+    lib().efwi_conv3d_set_kernel(1 if form == "tcgen05" else 0)
+
+
+def conv3d_status(device=None) -> bool:
+    """True when a tcgen05 convolution since the last call gave up waiting for
+    its tensor cores (its outputs are then incomplete); clears the flag."""
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    flag = C.c_int(0)
+    with torch.cuda.device(dev):
+        rc = lib().efwi_conv3d_status(C.byref(flag), _stream(dev))
+    if rc:
+        raise RuntimeError(f"efwi_conv3d_status failed ({rc})")
+    return bool(flag.value)
+
+
 def conv3d_wgrad(x: torch.Tensor, dy: torch.Tensor, nparts: int = 296) -> torch.Tensor:
     """dW[t][co][ci] = sum_v dy[v][co] x[v + off_t][ci] (f32)."""
     D, H, W = x.shape[:3]
