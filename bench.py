@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--nt", type=int, default=2000)
     ap.add_argument("--shots", type=int, default=16)
     ap.add_argument("--n", type=int, default=128, help="model cells per axis")
+    ap.add_argument("--conv-form", default="tcgen05-tma",
+                    help="convolution kernel of --case cnn's network: mma, tcgen05, tcgen05-tma")
     ap.add_argument("--profile-sample", type=int, default=16,
                     help="untimed profiling pass: time every k-th time step's launches "
                          "with CUDA events")
@@ -550,7 +552,7 @@ def run_cnn(a):
     x = torch.randn(a.n, a.n, a.n, 16, device="cuda", generator=g).to(torch.bfloat16)
     w = (0.2 * torch.randn(27, 16, 16, device="cuda", generator=g)).to(torch.bfloat16)
     forms = {}
-    for form in ("mma", "tcgen05"):
+    for form in ("mma", "tcgen05", "tcgen05-tma"):
         set_conv_kernel(form)
         for _ in range(3):
             conv3d_raw(x, w, None, True)
@@ -566,7 +568,7 @@ def run_cnn(a):
                        "gbs": by1 / (ms * 1e-3) / 1e9, "frac_hbm": by1 / (ms * 1e-3) / 1e9 / hbm}
     if conv3d_status():
         raise RuntimeError("a tcgen05 convolution timed out waiting for its tensor cores")
-    set_conv_kernel("tcgen05")
+    set_conv_kernel(a.conv_form)
     net = Preconditioner(cin=3, seed=0).cuda()
     feats = torch.randn(3, a.n, a.n, a.n, device="cuda")
     layers = len(net.w)
@@ -592,8 +594,9 @@ def run_cnn(a):
                       "fwd_bwd_tflops": 3 * fl / (all_ms * 1e-3) / 1e12,
                       "one_layer_bf16_relu": forms,
                       "peak_bf16_tflops": peak, "peak_hbm_gbs": hbm,
-                      "note": "network: tcgen05 forward and input-gradient convolutions, "
-                              "mma.sync weight gradient; FP32 accumulation"}))
+                      "network_form": a.conv_form,
+                      "note": "network: forward and input-gradient convolutions in the named "
+                              "form, mma.sync weight gradient; FP32 accumulation"}))
 
 
 def main():

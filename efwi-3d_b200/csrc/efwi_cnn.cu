@@ -20,6 +20,8 @@
 //   k_conv3d_wgrad   dW[t][co][ci] = sum_v dy[v][co] x[v + off_t][ci]: one
 //                    warp per tap, K = voxels (16 per mma), per-CTA partial
 //                    sums reduced in a fixed order by k_reduce_partials.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -376,19 +378,207 @@ k_conv3d_fwd_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__rest
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
 }
 
+
+// The same tile and MMAs with the input staged by bulk tensor copies, two
+// stages deep: while the tensor cores work on tile k and the warps drain its
+// accumulator, the copy engine fills the other stage with tile k+1.  The
+// tensor map views x as [D][H][W][2 halves][8 channels]; a box of
+// 8 x 1 x 10 x 18 x 3 is one channel-half plane of the staged tile in exactly
+// the layout above (zeros outside the volume), so each stage takes two
+// copies.  Half planes start 128-byte aligned.
+constexpr int kTc2Plane = (kTcPlane + 127) / 128 * 128;  // 8704
+constexpr int kTc2Stage = 2 * kTc2Plane;
+constexpr int kTc2Copy = 2 * kTcPlane;                     // bytes the two copies deliver
+constexpr int kTc2Smem = 2 * kTc2Stage + kTcWBytes + 128;  // + alignment slack
+
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int c0, int c1, int c2, int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(128)
+k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *__restrict__ w,
+                 const float *__restrict__ bias, int D, int H, int W, int relu,
+                 __nv_bfloat16 *__restrict__ yb, float *__restrict__ yf) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full[2];
+  __shared__ __align__(8) uint64_t mma_bar;
+  __shared__ uint32_t tmem_slot;
+  unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  unsigned char *swt = smem + 2 * kTc2Stage;  // [t][half][co] x 16 B
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntx = (W + kTcX - 1) / kTcX, nty = (H + kTcY - 1) / kTcY;
+  const long long ntiles = (long long)ntx * nty * D;
+  auto tile_origin = [&](long long tile, int &x0, int &y0, int &z) {
+    x0 = (int)(tile % ntx) * kTcX;
+    const long long r = tile / ntx;
+    y0 = (int)(r % nty) * kTcY;
+    z = (int)(r / nty);
+  };
+  auto issue = [&](long long tile, int s) {  // thread 0: both half planes of a tile
+    int x0, y0, z;
+    tile_origin(tile, x0, y0, z);
+    mbar_arrive_expect_tx(&full[s], kTc2Copy);
+    unsigned char *dst = smem + s * kTc2Stage;
+    tma_load_5d(dst, &xmap, &full[s], 0, 0, x0 - 1, y0 - 1, z - 1);
+    tma_load_5d(dst + kTc2Plane, &xmap, &full[s], 0, 1, x0 - 1, y0 - 1, z - 1);
+  };
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&mma_bar, 1);
+    fence_mbar_init();
+    if ((long long)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+  }
+  for (int k = tid; k < 27 * 2 * kC; k += blockDim.x) {
+    const int t = k / (2 * kC), r = k % (2 * kC), h = r / kC, co = r % kC;
+    *reinterpret_cast<uint4 *>(swt + ((t * 2 + h) * kC + co) * 16) =
+        *reinterpret_cast<const uint4 *>(w + (t * kC + co) * kC + h * 8);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(
+                     smem_u32(&tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async_smem();  // the staged weights are read by the tensor cores
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t swa = smem_u32(swt);
+  bool ok = true;
+  int pending = -1;  // stage whose copies thread 0 issued and nobody waited for yet
+  if (tid == 0 && (long long)blockIdx.x < ntiles) pending = 0;
+  int k = 0;
+  for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++k) {
+    const int s = k & 1;
+    bool mine = true;  // thread 0: the stage's copies arrived
+    if (tid == 0) {
+      const long long next = tile + gridDim.x;
+      if (next < ntiles) {  // stage s^1 was last read by tile k-1's MMAs, which completed
+        issue(next, s ^ 1);
+      }
+      mine = mbar_wait_bounded(&full[s], (uint32_t)((k >> 1) & 1));
+      pending = next < ntiles ? (s ^ 1) : -1;
+      if (mine) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t sxa = smem_u32(smem + s * kTc2Stage);
+#pragma unroll 1
+        for (int t = 0; t < 27; ++t) {
+          const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+          const uint32_t a = sxa + (uint32_t)(((dz * kTcSY + dy) * kTcSX + dx) * 16);
+          const uint64_t ad = tc_desc(a, kTc2Plane, kTcSX * 16);
+          const uint64_t bd = tc_desc(swa + (uint32_t)(t * 2 * kC * 16), kC * 16, 8 * 16);
+          tc_mma(tmem, ad, bd, t > 0 ? 1u : 0u);
+        }
+      }
+      tc_commit(&mma_bar);  // with no MMA issued it completes at once
+    }
+    const bool got =
+        __syncthreads_and(mbar_wait_bounded(&mma_bar, (uint32_t)(k & 1)) && mine);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (got) {
+      int x0, y0, z;
+      tile_origin(tile, x0, y0, z);
+      float v[16];
+      tc_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
+      const int m = warp * 32 + lane;
+      const int xv = x0 + (m & 7), yv = y0 + (m >> 3);
+      if (xv < W && yv < H) {
+        const long long off = (((long long)z * H + yv) * W + xv) * kC;
+        float o[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          o[q] = v[q] + (bias ? bias[q] : 0.f);
+          if (relu) o[q] = fmaxf(o[q], 0.f);
+        }
+        if (yb) {
+          uint32_t pk[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(o[2 * q], o[2 * q + 1]);
+            pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+          }
+          uint4 *dst = reinterpret_cast<uint4 *>(yb + off);
+          dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        }
+        if (yf) {
+          float4 *dst = reinterpret_cast<float4 *>(yf + off);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            dst[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // TMEM is free again
+    ok = got;
+  }
+  if (!ok && tid == 0) {
+    atomicExch(&g_conv_status, EFWI_STATUS_TIMEOUT);
+    // bounded waits for what may still be in flight: the last MMAs and the
+    // copies of the prefetched stage
+    mbar_wait_bounded(&mma_bar, (uint32_t)((k - 1) & 1));
+    mbar_wait_bounded(&full[(k - 1) & 1], (uint32_t)(((k - 1) >> 1) & 1));
+    if (pending >= 0) mbar_wait_bounded(&full[pending], (uint32_t)((k >> 1) & 1));
+  }
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+}
+
 }  // namespace
 }  // namespace efwi
 
 using namespace efwi;
 
 namespace {
-std::atomic<int> g_conv_kernel{0};  // 1: tcgen05 form, 0: mma.sync form
-std::atomic<unsigned long long> g_tc_smem_set{0};
+// 0: mma.sync; 1: tcgen05, tile staged by loads; 2: tcgen05, tiles staged by
+// bulk tensor copies two stages deep
+std::atomic<int> g_conv_kernel{0};
+std::atomic<unsigned long long> g_tc_smem_set{0}, g_tc2_smem_set{0};
 int g_sm_count[64] = {0};
+std::atomic<PFN_cuTensorMapEncodeTiled_v12000> g_conv_encode{nullptr};
+
+PFN_cuTensorMapEncodeTiled_v12000 conv_encoder() {
+  PFN_cuTensorMapEncodeTiled_v12000 f = g_conv_encode.load();
+  if (f) return f;
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn)
+    return nullptr;
+  f = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  g_conv_encode.store(f);
+  return f;
+}
+
+// x [D][H][W][16] bf16 as a 5-D tensor (8 channels, 2 halves, W, H, D) with
+// boxes of one channel half over the 10 x 18 x 3 staged voxels.
+bool conv_map(CUtensorMap *m, const void *x, int D, int H, int W) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = conv_encoder();
+  if (!enc) return false;
+  cuuint64_t dims[5] = {8, 2, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D};
+  cuuint64_t strides[4] = {16, 32, 32ull * W, 32ull * W * H};
+  cuuint32_t box[5] = {8, 1, (cuuint32_t)kTcSX, (cuuint32_t)kTcSY, 3};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(x), dims, strides, box,
+             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 }  // namespace
 
-extern "C" int efwi_conv3d_set_kernel(int tcgen05) {
-  g_conv_kernel.store(tcgen05 ? 1 : 0);
+extern "C" int efwi_conv3d_set_kernel(int form) {
+  if (form < 0 || form > 2) return 1;
+  g_conv_kernel.store(form);
   return 0;
 }
 
@@ -411,19 +601,29 @@ extern "C" int efwi_conv3d_forward(const void *x, const void *w, const float *bi
   if (!x || !w || D < 1 || H < 1 || W < 1 || D > 65535 || (!y_bf16 && !y_f32)) return 1;
   if (((uintptr_t)x & 15) != 0) return 1;  // staged with 16-byte loads
   cudaStream_t st = (cudaStream_t)stream;
-  if (g_conv_kernel.load() == 1 && ((uintptr_t)w & 15) == 0 && ((uintptr_t)y_bf16 & 15) == 0 &&
+  const int form = g_conv_kernel.load();
+  if (form != 0 && ((uintptr_t)w & 15) == 0 && ((uintptr_t)y_bf16 & 15) == 0 &&
       ((uintptr_t)y_f32 & 15) == 0) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 2;
     int &sms = g_sm_count[dev & 63];
     if (!sms && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       return 2;
-    set_smem_once(k_conv3d_fwd_tc, kTcSmem, g_tc_smem_set);
     const long long tiles = (long long)((W + kTcX - 1) / kTcX) * ((H + kTcY - 1) / kTcY) * D;
-    const int blocks = (int)std::min<long long>(tiles, 6LL * sms);
-    k_conv3d_fwd_tc<<<blocks, 128, kTcSmem, st>>>((const __nv_bfloat16 *)x,
-                                                  (const __nv_bfloat16 *)w, bias, D, H, W, relu,
-                                                  (__nv_bfloat16 *)y_bf16, y_f32);
+    if (form == 2) {
+      CUtensorMap map;
+      if (!conv_map(&map, x, D, H, W)) return 2;
+      set_smem_once(k_conv3d_fwd_tc2, kTc2Smem, g_tc2_smem_set);
+      const int blocks = (int)std::min<long long>(tiles, 4LL * sms);
+      k_conv3d_fwd_tc2<<<blocks, 128, kTc2Smem, st>>>(map, (const __nv_bfloat16 *)w, bias, D, H,
+                                                      W, relu, (__nv_bfloat16 *)y_bf16, y_f32);
+    } else {
+      set_smem_once(k_conv3d_fwd_tc, kTcSmem, g_tc_smem_set);
+      const int blocks = (int)std::min<long long>(tiles, 6LL * sms);
+      k_conv3d_fwd_tc<<<blocks, 128, kTcSmem, st>>>((const __nv_bfloat16 *)x,
+                                                    (const __nv_bfloat16 *)w, bias, D, H, W, relu,
+                                                    (__nv_bfloat16 *)y_bf16, y_f32);
+    }
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
   }
   const dim3 grid((W + kTileX - 1) / kTileX, (H + kRowsFwd - 1) / kRowsFwd, D);

@@ -43,13 +43,17 @@ def conv3d_raw(x: torch.Tensor, wb: torch.Tensor, bias, relu: bool, out_f32: boo
     return yf if out_f32 else yb
 
 
+CONV_FORMS = {"mma": 0, "tcgen05": 1, "tcgen05-tma": 2}
+
+
 def set_conv_kernel(form: str) -> None:
-    """'tcgen05' (tensor-memory accumulator, one MMA per tap for 128 voxels)
-    or 'mma' (mma.sync m16n8k16) for every later forward / input-gradient
-    convolution of this process."""
-    if form not in ("tcgen05", "mma"):
+    """Kernel of every later forward / input-gradient convolution of this
+    process: 'mma' (mma.sync m16n8k16), 'tcgen05' (tensor-memory accumulator,
+    one MMA per tap for 128 voxels, tile staged by loads) or 'tcgen05-tma'
+    (the same MMAs, tiles staged by bulk tensor copies two stages deep)."""
+    if form not in CONV_FORMS:
         raise ValueError(f"unknown convolution kernel form {form!r}")
-    lib().efwi_conv3d_set_kernel(1 if form == "tcgen05" else 0)
+    lib().efwi_conv3d_set_kernel(CONV_FORMS[form])
 
 
 def conv3d_status(device=None) -> bool:

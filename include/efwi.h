@@ -275,14 +275,16 @@ int efwi_conv3d_forward(const void *x, const void *w, const float *bias, int D, 
                         int relu, void *y_bf16, float *y_f32, void *stream);
 int efwi_conv3d_wgrad(const void *x, const void *dy, int D, int H, int W, float *partial,
                       int nparts, float *dw, void *stream);
-/* Kernel form of efwi_conv3d_forward for this process: 1 = tcgen05.mma with
- * the accumulator in tensor memory (128 voxels x 16 channels per tile, one
- * MMA per tap), 0 = mma.sync.  Both give the same sums up to FP32 rounding
- * order.  The tcgen05 form needs w and the outputs 16-byte aligned and falls
- * back to mma.sync otherwise.  efwi_conv3d_status reads and clears the flag
- * the tcgen05 form sets when its bounded wait for the tensor cores ran out
- * (the call's outputs are then incomplete). */
-int efwi_conv3d_set_kernel(int tcgen05);
+/* Kernel form of efwi_conv3d_forward for this process: 0 = mma.sync;
+ * 1 = tcgen05.mma with the accumulator in tensor memory (128 voxels x 16
+ * channels per tile, one MMA per tap), tile staged by loads; 2 = the same
+ * MMAs with the tiles staged by bulk tensor copies two stages deep.  All
+ * give the same sums up to FP32 rounding order.  The tcgen05 forms need w
+ * and the outputs 16-byte aligned and fall back to mma.sync otherwise.
+ * Returns 1 for an unknown form.  efwi_conv3d_status reads and clears the
+ * flag the tcgen05 forms set when a bounded wait for the tensor cores or
+ * the copies ran out (the call's outputs are then incomplete). */
+int efwi_conv3d_set_kernel(int form);
 int efwi_conv3d_status(int *timed_out, void *stream);
 
 /* Per-kernel timing with CUDA events on the call's stream (every

@@ -9,6 +9,7 @@ import torch.nn.functional as F
 from helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
+DEFAULT_FORM = "mma"
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -44,8 +45,9 @@ def test_forward_matches_torch(shape, relu):
     assert rel_l2(ours_b.float().cpu(), ref.cpu()) < 1e-2
 
 
+@pytest.mark.parametrize("form_tc", ["tcgen05", "tcgen05-tma"])
 @pytest.mark.parametrize("shape", [(1, 1, 1), (3, 17, 9), (4, 33, 70), (2, 16, 8)])
-def test_tcgen05_form_matches_mma_form_and_torch(shape):
+def test_tcgen05_form_matches_mma_form_and_torch(shape, form_tc):
     """The tcgen05 convolution (accumulator in tensor memory) against the
     mma.sync one and torch, on tiles cut at every edge (8 x 16 voxel tiles)."""
     from efwi.cnn import conv3d_raw, conv3d_status, set_conv_kernel
@@ -53,20 +55,21 @@ def test_tcgen05_form_matches_mma_form_and_torch(shape):
     x = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
     w = (0.2 * torch.randn(27, 16, 16, device="cuda", generator=g)).to(torch.bfloat16)
     b = torch.randn(16, device="cuda", generator=g)
+    ref = torch.relu(F.conv3d(_ncdhw(x), _torch_w(w), b, padding=1))[0].permute(1, 2, 3, 0)
     try:
         set_conv_kernel("mma")
         mma = conv3d_raw(x, w, b, True, out_f32=True)
-        set_conv_kernel("tcgen05")
-        tc = conv3d_raw(x, w, b, True, out_f32=True)
-        tcb = conv3d_raw(x, w, b, True)
-        torch.cuda.synchronize()
-        assert not conv3d_status()
+        for form in (form_tc,):
+            set_conv_kernel(form)
+            tc = conv3d_raw(x, w, b, True, out_f32=True)
+            tcb = conv3d_raw(x, w, b, True)
+            torch.cuda.synchronize()
+            assert not conv3d_status()
+            assert rel_l2(tc.cpu(), ref.cpu()) < 1e-5, form
+            assert rel_l2(tc.cpu(), mma.cpu()) < 1e-5, form
+            assert rel_l2(tcb.float().cpu(), ref.cpu()) < 1e-2, form
     finally:
-        set_conv_kernel("tcgen05")
-    ref = torch.relu(F.conv3d(_ncdhw(x), _torch_w(w), b, padding=1))[0].permute(1, 2, 3, 0)
-    assert rel_l2(tc.cpu(), ref.cpu()) < 1e-5
-    assert rel_l2(tc.cpu(), mma.cpu()) < 1e-5
-    assert rel_l2(tcb.float().cpu(), ref.cpu()) < 1e-2
+        set_conv_kernel(DEFAULT_FORM)
 
 
 def test_input_and_weight_gradients_match_torch():
