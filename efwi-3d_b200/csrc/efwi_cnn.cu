@@ -379,17 +379,19 @@ k_conv3d_fwd_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__rest
 }
 
 
-// The same tile and MMAs with the input staged by bulk tensor copies, two
-// stages deep: while the tensor cores work on tile k and the warps drain its
-// accumulator, the copy engine fills the other stage with tile k+1.  The
-// tensor map views x as [D][H][W][2 halves][8 channels]; a box of
+// The same tile and MMAs with the input staged by bulk tensor copies and
+// the work software-pipelined: while the warps drain tile j's accumulator,
+// the tensor cores already work on tile j+1 (two accumulators of 16 TMEM
+// columns, used in turn) and the copy engine fills a third stage with tile
+// j+2.  The tensor map views x as [D][H][W][2 halves][8 channels]; a box of
 // 8 x 1 x 10 x 18 x 3 is one channel-half plane of the staged tile in exactly
 // the layout above (zeros outside the volume), so each stage takes two
 // copies.  Half planes start 128-byte aligned.
 constexpr int kTc2Plane = (kTcPlane + 127) / 128 * 128;  // 8704
 constexpr int kTc2Stage = 2 * kTc2Plane;
-constexpr int kTc2Copy = 2 * kTcPlane;                     // bytes the two copies deliver
-constexpr int kTc2Smem = 2 * kTc2Stage + kTcWBytes + 128;  // + alignment slack
+constexpr int kTc2Stages = 3;
+constexpr int kTc2Copy = 2 * kTcPlane;  // bytes the two copies deliver
+constexpr int kTc2Smem = kTc2Stages * kTc2Stage + kTcWBytes + 128;  // + alignment slack
 
 __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, uint64_t *bar,
                                             int c0, int c1, int c2, int c3, int c4) {
@@ -406,34 +408,63 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
                  const float *__restrict__ bias, int D, int H, int W, int relu,
                  __nv_bfloat16 *__restrict__ yb, float *__restrict__ yf) {
   extern __shared__ unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full[2];
-  __shared__ __align__(8) uint64_t mma_bar;
+  __shared__ __align__(8) uint64_t full[kTc2Stages];  // stage filled (copies landed)
+  __shared__ __align__(8) uint64_t done[2];           // accumulator b complete
   __shared__ uint32_t tmem_slot;
+  __shared__ int s_abort;
   unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  unsigned char *swt = smem + 2 * kTc2Stage;  // [t][half][co] x 16 B
+  unsigned char *swt = smem + kTc2Stages * kTc2Stage;  // [t][half][co] x 16 B
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntx = (W + kTcX - 1) / kTcX, nty = (H + kTcY - 1) / kTcY;
   const long long ntiles = (long long)ntx * nty * D;
-  auto tile_origin = [&](long long tile, int &x0, int &y0, int &z) {
+  // tiles of this CTA: blockIdx.x + j * gridDim.x, j < nj
+  const long long nj =
+      (long long)blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto tile_origin = [&](long long j, int &x0, int &y0, int &z) {
+    const long long tile = blockIdx.x + j * gridDim.x;
     x0 = (int)(tile % ntx) * kTcX;
     const long long r = tile / ntx;
     y0 = (int)(r % nty) * kTcY;
     z = (int)(r / nty);
   };
-  auto issue = [&](long long tile, int s) {  // thread 0: both half planes of a tile
+  const uint32_t swa = smem_u32(swt);
+  uint32_t tmem = 0;
+  // thread 0: copies of tile j into stage j % 3
+  auto issue = [&](long long j) {
     int x0, y0, z;
-    tile_origin(tile, x0, y0, z);
+    tile_origin(j, x0, y0, z);
+    const int s = (int)(j % kTc2Stages);
     mbar_arrive_expect_tx(&full[s], kTc2Copy);
     unsigned char *dst = smem + s * kTc2Stage;
     tma_load_5d(dst, &xmap, &full[s], 0, 0, x0 - 1, y0 - 1, z - 1);
     tma_load_5d(dst + kTc2Plane, &xmap, &full[s], 0, 1, x0 - 1, y0 - 1, z - 1);
   };
+  // thread 0: the 27 MMAs of tile j into accumulator j & 1, once its stage landed
+  auto mma = [&](long long j) -> bool {
+    const int s = (int)(j % kTc2Stages);
+    if (!mbar_wait_bounded(&full[s], (uint32_t)((j / kTc2Stages) & 1))) return false;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t sxa = smem_u32(smem + s * kTc2Stage);
+    const uint32_t d = tmem + (uint32_t)((j & 1) * kC);
+#pragma unroll 1
+    for (int t = 0; t < 27; ++t) {
+      const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+      const uint32_t a = sxa + (uint32_t)(((dz * kTcSY + dy) * kTcSX + dx) * 16);
+      const uint64_t ad = tc_desc(a, kTc2Plane, kTcSX * 16);
+      const uint64_t bd = tc_desc(swa + (uint32_t)(t * 2 * kC * 16), kC * 16, 8 * 16);
+      tc_mma(d, ad, bd, t > 0 ? 1u : 0u);
+    }
+    tc_commit(&done[j & 1]);
+    return true;
+  };
+  long long n_tma = 0, n_mma = 0;  // thread 0: tiles whose copies / MMAs were issued
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&mma_bar, 1);
+    for (int s = 0; s < kTc2Stages; ++s) mbar_init(&full[s], 1);
+    mbar_init(&done[0], 1);
+    mbar_init(&done[1], 1);
     fence_mbar_init();
-    if ((long long)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    s_abort = 0;
+    for (; n_tma < 2 && n_tma < nj; ++n_tma) issue(n_tma);
   }
   for (int k = tid; k < 27 * 2 * kC; k += blockDim.x) {
     const int t = k / (2 * kC), r = k % (2 * kC), h = r / kC, co = r % kC;
@@ -450,44 +481,35 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tmem = tmem_slot;
-  const uint32_t swa = smem_u32(swt);
-  bool ok = true;
-  int pending = -1;  // stage whose copies thread 0 issued and nobody waited for yet
-  if (tid == 0 && (long long)blockIdx.x < ntiles) pending = 0;
-  int k = 0;
-  for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++k) {
-    const int s = k & 1;
-    bool mine = true;  // thread 0: the stage's copies arrived
-    if (tid == 0) {
-      const long long next = tile + gridDim.x;
-      if (next < ntiles) {  // stage s^1 was last read by tile k-1's MMAs, which completed
-        issue(next, s ^ 1);
+  tmem = tmem_slot;
+  if (tid == 0 && nj > 0) {
+    if (mma(0)) n_mma = 1;
+    else s_abort = 1;
+  }
+  __syncthreads();
+  bool ok = !s_abort;
+  for (long long j = 0; j < nj && ok; ++j) {
+    if (tid == 0 && !s_abort) {
+      // accumulator (j+1)&1 was drained in iteration j-1; stage (j+2)%3 was
+      // last read by tile j-1's MMAs, which completed before that drain
+      if (j + 1 < nj) {
+        if (mma(j + 1)) n_mma = j + 2;
+        else s_abort = 1;
       }
-      mine = mbar_wait_bounded(&full[s], (uint32_t)((k >> 1) & 1));
-      pending = next < ntiles ? (s ^ 1) : -1;
-      if (mine) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t sxa = smem_u32(smem + s * kTc2Stage);
-#pragma unroll 1
-        for (int t = 0; t < 27; ++t) {
-          const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-          const uint32_t a = sxa + (uint32_t)(((dz * kTcSY + dy) * kTcSX + dx) * 16);
-          const uint64_t ad = tc_desc(a, kTc2Plane, kTcSX * 16);
-          const uint64_t bd = tc_desc(swa + (uint32_t)(t * 2 * kC * 16), kC * 16, 8 * 16);
-          tc_mma(tmem, ad, bd, t > 0 ? 1u : 0u);
-        }
+      if (!s_abort && j + 2 < nj) {
+        issue(j + 2);
+        n_tma = j + 3;
       }
-      tc_commit(&mma_bar);  // with no MMA issued it completes at once
     }
+    // every thread takes the same branch: tcgen05.ld is warp-collective
     const bool got =
-        __syncthreads_and(mbar_wait_bounded(&mma_bar, (uint32_t)(k & 1)) && mine);
+        __syncthreads_and(mbar_wait_bounded(&done[j & 1], (uint32_t)((j >> 1) & 1)));
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (got) {
       int x0, y0, z;
-      tile_origin(tile, x0, y0, z);
+      tile_origin(j, x0, y0, z);
       float v[16];
-      tc_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
+      tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((j & 1) * kC), v);
       const int m = warp * 32 + lane;
       const int xv = x0 + (m & 7), yv = y0 + (m >> 3);
       if (xv < W && yv < H) {
@@ -518,16 +540,16 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();  // TMEM is free again
-    ok = got;
+    __syncthreads();  // accumulator j & 1 is free again; s_abort is published
+    ok = got && !s_abort;
   }
   if (!ok && tid == 0) {
     atomicExch(&g_conv_status, EFWI_STATUS_TIMEOUT);
-    // bounded waits for what may still be in flight: the last MMAs and the
-    // copies of the prefetched stage
-    mbar_wait_bounded(&mma_bar, (uint32_t)((k - 1) & 1));
-    mbar_wait_bounded(&full[(k - 1) & 1], (uint32_t)(((k - 1) >> 1) & 1));
-    if (pending >= 0) mbar_wait_bounded(&full[pending], (uint32_t)((k >> 1) & 1));
+    // bounded waits for what may still be in flight: the copies of tiles
+    // whose MMAs were never issued, and the last MMAs issued
+    for (long long j = n_mma; j < n_tma; ++j)
+      mbar_wait_bounded(&full[j % kTc2Stages], (uint32_t)((j / kTc2Stages) & 1));
+    if (n_mma > 0) mbar_wait_bounded(&done[(n_mma - 1) & 1], (uint32_t)(((n_mma - 1) >> 1) & 1));
   }
   __syncthreads();
   if (warp == 0)
@@ -542,7 +564,7 @@ using namespace efwi;
 namespace {
 // 0: mma.sync; 1: tcgen05, tile staged by loads; 2: tcgen05, tiles staged by
 // bulk tensor copies two stages deep
-std::atomic<int> g_conv_kernel{0};
+std::atomic<int> g_conv_kernel{2};
 std::atomic<unsigned long long> g_tc_smem_set{0}, g_tc2_smem_set{0};
 int g_sm_count[64] = {0};
 std::atomic<PFN_cuTensorMapEncodeTiled_v12000> g_conv_encode{nullptr};
@@ -614,7 +636,7 @@ extern "C" int efwi_conv3d_forward(const void *x, const void *w, const float *bi
       CUtensorMap map;
       if (!conv_map(&map, x, D, H, W)) return 2;
       set_smem_once(k_conv3d_fwd_tc2, kTc2Smem, g_tc2_smem_set);
-      const int blocks = (int)std::min<long long>(tiles, 4LL * sms);
+      const int blocks = (int)std::min<long long>(tiles, 3LL * sms);  // 66 KB of shared memory each
       k_conv3d_fwd_tc2<<<blocks, 128, kTc2Smem, st>>>(map, (const __nv_bfloat16 *)w, bias, D, H,
                                                       W, relu, (__nv_bfloat16 *)y_bf16, y_f32);
     } else {

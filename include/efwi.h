@@ -283,7 +283,7 @@ int efwi_conv3d_wgrad(const void *x, const void *dy, int D, int H, int W, float 
  * and the outputs 16-byte aligned and fall back to mma.sync otherwise.
  * Returns 1 for an unknown form.  efwi_conv3d_status reads and clears the
  * flag the tcgen05 forms set when a bounded wait for the tensor cores or
- * the copies ran out (the call's outputs are then incomplete). */
+ * the copies ran out (the call's outputs are then incomplete).  Default 2. */
 int efwi_conv3d_set_kernel(int form);
 int efwi_conv3d_status(int *timed_out, void *stream);
 

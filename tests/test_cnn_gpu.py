@@ -9,7 +9,7 @@ import torch.nn.functional as F
 from helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
-DEFAULT_FORM = "mma"
+DEFAULT_FORM = "tcgen05-tma"
 
 
 @pytest.fixture(scope="module", autouse=True)
