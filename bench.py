@@ -187,8 +187,9 @@ def kernel_bytes(grid, nshot_launch=1):
 # padded grid (128^3 model, C-PML 12), one shot per launch, from one ncu
 # capture of each kernel (dram__bytes_read.sum + dram__bytes_write.sum);
 # other grids report no traffic.
-TRAFFIC_152 = {"rev_velocity": 415.4e6, "rev_stress": 501.3e6,
-               "stress_fwd": 221.6e6, "velocity_fwd": 184.4e6}
+TRAFFIC_152 = {"rev_velocity": 423.3e6, "rev_stress": 514.7e6,
+               "stress_fwd": 236.5e6, "velocity_fwd": 185.5e6,
+               "adj_velocity": 356.6e6, "adj_stress": 324.9e6}
 
 
 def algorithmic_step_bytes(grid, nmodel):
