@@ -65,6 +65,9 @@ def parse():
                          "L1 stencils (default 4)")
     ap.add_argument("--zchunk", type=int, default=8)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
+    ap.add_argument("--no-graphs", dest="graphs", action="store_false",
+                    help="launch the time loops' kernels one by one instead of replaying "
+                         "captured CUDA graphs (same kernels, same work)")
     ap.add_argument("--mode", default="reference", choices=["reference", "exact"],
                     help="gradient algorithm: the reference's (headline) or the exact "
                          "discrete adjoint with binomial checkpoints")
@@ -644,6 +647,7 @@ def main():
     bx = a.tile_bx or (8 if a.mode == "exact" else 4)
     P = Propagator(g, device=dev, tile_bx=bx, zchunk=a.zchunk, max_batch=4)
     P.set_lanes(a.lanes)
+    P.set_graphs(a.graphs)
     P.set_checkpoint_budget(int(a.ck_budget * (1 << 30)))
     P.set_survey(prob.shots, prob.stf)
     lt, mt, rt = prob.params("true")
@@ -796,7 +800,7 @@ def main():
                                        f" {len(ids)} shots per GPU, nt={g.nt}, {a.mode} gradient",
                            "model_cells": a.n, "padded": g.nz, "shots_per_gpu": len(ids),
                            "nt": g.nt, "mode": a.mode,
-                           "lanes": a.lanes,
+                           "lanes": a.lanes, "graphs": a.graphs,
                            "checkpoints": ck_stats,
                            "checkpoint_budget_gib": a.ck_budget if a.mode == "exact" else None,
                            "l2": "inputs larger than L2 (9 fields x 14 MB per shot + shell store)",
