@@ -137,9 +137,15 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
   }
   const int off = (ty + TMA_HX) * TMA_BOXY + tx + TMA_HY;
   const int pt = ty * 32 + tx;
+  // row entry of the shell map and receiver-plane index, one plane ahead
+  const bool use_shell = L::REV && shell.rows && act, use_inj = L::ADJ && inj.a.plane;
+  int srow = use_shell ? shell.rows[z0 * nx + x] : -1;
+  int rmap = use_inj ? inj.a.plane[z0] : -1;
 
   for (int q = 0; q < nq; ++q, i += sz) {
     const int z = z0 + q;
+    const int srow_n = (use_shell && q + 1 < nq) ? shell.rows[(z + 1) * nx + x] : -1;
+    const int rmap_n = (use_inj && q + 1 < nq) ? inj.a.plane[z + 1] : -1;
     float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f, h6 = 0.f, h7 = 0.f;
     if (act && q + 1 < nq) {
       if (L::REV) { h0 = f.szz[i + 3 * sz]; h1 = f.sxz[i + 2 * sz]; h2 = f.syz[i + 2 * sz]; }
@@ -162,15 +168,14 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
     // receiver map index (res_injection)
     int sk = -1;
     float rvz = 0.f, rvx = 0.f, rvy = 0.f;
-    if (L::REV && shell.rows && act) {
-      sk = shell_index(shell, shell.rows[z * nx + x], y);
+    if (use_shell) {
+      sk = shell_index(shell, srow, y);
       if (sk >= 0) {
         const int n = shell.npts;
         rvz = shell.store[6 * n + sk]; rvx = shell.store[7 * n + sk];
         rvy = shell.store[8 * n + sk];
       }
     }
-    const int rmap = (L::ADJ && inj.a.plane) ? inj.a.plane[z] : -1;
     const bool got = ring.wait(q);
     if (act && got) {
       const float b = ring.point(q, L::MB)[pt];
@@ -274,6 +279,8 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
     }
     szz.shift(h0); sxz.shift(h1); syz.shift(h2); aszz.shift(h3);
     asxx.shift(h4); asyy.shift(h5); asxz.shift(h6); asyz.shift(h7);
+    srow = srow_n;
+    rmap = rmap_n;
     if (__syncthreads_or(!got)) {
       ring_abort(ring, q, nq, R, tid, status);
       return;
@@ -333,9 +340,13 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
   }
   const int off = (ty + TMA_HX) * TMA_BOXY + tx + TMA_HY;
   const int pt = ty * 32 + tx;
+  // row entry of the shell map, one plane ahead
+  const bool use_shell = shell.rows && act;
+  int srow = use_shell ? shell.rows[z0 * nx + x] : -1;
 
   for (int q = 0; q < nq; ++q, i += sz) {
     const int z = z0 + q;
+    const int srow_n = (use_shell && q + 1 < nq) ? shell.rows[(z + 1) * nx + x] : -1;
     float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f;
     if (act && q + 1 < nq) {
       h0 = f.vz[i + 2 * sz]; h1 = f.vx[i + 3 * sz]; h2 = f.vy[i + 3 * sz];
@@ -349,8 +360,8 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
     // wait so that their latency overlaps it
     int sk = -1;
     float rst[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (shell.rows && act) {
-      sk = shell_index(shell, shell.rows[z * nx + x], y);
+    if (use_shell) {
+      sk = shell_index(shell, srow, y);
       if (sk >= 0) {
 #pragma unroll
         for (int k = 0; k < 6; ++k) rst[k] = shell.store[k * shell.npts + sk];
@@ -461,6 +472,7 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
       }
     }
     vz.shift(h0); vx.shift(h1); vy.shift(h2); avz.shift(h3); avx.shift(h4); avy.shift(h5);
+    srow = srow_n;
     if (__syncthreads_or(!got)) {
       ring_abort(ring, q, nq, R, tid, status);
       return;
