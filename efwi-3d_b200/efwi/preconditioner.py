@@ -238,6 +238,12 @@ def _sync(dev) -> None:
         torch.cuda.synchronize(dev)
 
 
+def _dot(a: torch.Tensor, b: torch.Tensor) -> float:
+    """Inner product in FP64: misfit gradients of FP32 volumes can be small
+    enough (1e-20 and below per cell) that their squares underflow FP32."""
+    return float(torch.sum(a.double() * b.double()))
+
+
 def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10,
           net=None, first_step: float = 20.0, c1: float = 1e-4, max_trials: int = 12,
           max_expand: int = 3, learned_trials: int = 4,
@@ -278,31 +284,31 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
         q = q.clone()
         al = []
         for s, y in reversed(list(zip(S, Y))):
-            rho = 1.0 / torch.sum(y * s)
-            a = rho * torch.sum(s * q)
+            rho = 1.0 / _dot(y, s)
+            a = rho * _dot(s, q)
             q -= a * y
             al.append((rho, a))
         if h0 is not None:
             nq = h0(q)
             if S:
-                yn = torch.sum(Y[-1] * h0(Y[-1]))
+                yn = _dot(Y[-1], h0(Y[-1]))
                 if not float(yn) > 0:
                     return None  # the map is not positive along y: no learned H0
-                r = (torch.sum(S[-1] * Y[-1]) / yn) * nq
+                r = (_dot(S[-1], Y[-1]) / yn) * nq
             else:
                 r = nq * (first_step / (nq.abs().max() + 1e-30))
         elif S:
-            gamma = torch.sum(S[-1] * Y[-1]) / torch.sum(Y[-1] * Y[-1])
+            gamma = _dot(S[-1], Y[-1]) / _dot(Y[-1], Y[-1])
             r = gamma * q
         else:
             r = q * (first_step / (q.abs().max() + 1e-30))
         for (s, y), (rho, a) in zip(zip(S, Y), reversed(al)):
-            b = rho * torch.sum(y * r)
+            b = rho * _dot(y, r)
             r += s * (a - b)
         return -r
 
     def search(d, J, g, trials):
-        gd = float(torch.sum(g * d))
+        gd = _dot(g, d)
         if not gd < 0:
             return None
         alpha = 1.0
@@ -343,7 +349,7 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
             break
         vn, Jn, gn = step
         s, y = vn - vp, gn - g
-        if float(torch.sum(s * y)) > 1e-12 * float(torch.sum(y * y)):
+        if _dot(s, y) > 1e-12 * _dot(y, y):
             S.append(s)
             Y.append(y)
             if len(S) > memory:

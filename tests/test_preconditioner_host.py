@@ -85,3 +85,27 @@ def test_net_mode_is_checked():
     with pytest.raises(ValueError):
         lbfgs(_Quadratic(), torch.full((12, 12, 12), 2500.0, dtype=torch.float64), iters=1,
               net_mode="other")
+
+
+class _TinyQuadratic(_Quadratic):
+    """The same objective in FP32 with the misfit scaled by 1e-27, about as small
+    as the misfit gradients of the elastic problem get per cell: squares of
+    the gradient entries underflow FP32."""
+
+    SCALE = 1e-27
+
+    def __init__(self):
+        super().__init__()
+        self.h = (self.h * self.SCALE).float()
+        self.vp_true = self.vp_true.float()
+
+
+def test_lbfgs_steps_on_gradients_whose_squares_underflow_fp32():
+    import torch
+    from efwi.preconditioner import lbfgs
+    obj = _TinyQuadratic()
+    g0 = obj.value_and_grad(torch.full_like(obj.vp_true, 2500.0))[1]
+    assert float(torch.sum(g0 * g0)) == 0.0  # the FP32 inner product underflows
+    res = lbfgs(obj, torch.full_like(obj.vp_true, 2500.0), iters=6)
+    assert len(res.misfit) == 7
+    assert res.misfit[-1] < 0.5 * res.misfit[0]
