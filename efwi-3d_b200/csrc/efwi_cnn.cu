@@ -266,6 +266,23 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16]) {
 
 __device__ int g_conv_status;  // EFWI_STATUS_TIMEOUT after a wait that ran out
 
+// The 27 MMAs of one tile into the accumulator at TMEM address d: the
+// descriptors of tap t are the tap-0 ones with the start address moved by
+// the tap's offset (the 14-bit start field cannot carry: shared addresses
+// stay below 256 KB), so the unrolled loop issues one add per operand.
+__device__ __forceinline__ void tc_tile_mmas(uint32_t d, uint32_t sxa, uint32_t plane_bytes,
+                                             uint32_t swa) {
+  const uint64_t a0 = tc_desc(sxa, plane_bytes, kTcSX * 16);
+  const uint64_t b0 = tc_desc(swa, kC * 16, 8 * 16);
+#pragma unroll
+  for (int t = 0; t < 27; ++t) {
+    const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+    const uint64_t ao = (uint64_t)((dz * kTcSY + dy) * kTcSX + dx);  // 16-byte units
+    const uint64_t bo = (uint64_t)(t * 2 * kC);                      // 16-byte units
+    tc_mma(d, a0 + ao, b0 + bo, t > 0 ? 1u : 0u);
+  }
+}
+
 __global__ void __launch_bounds__(128)
 k_conv3d_fwd_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
                 const float *__restrict__ bias, int D, int H, int W, int relu,
@@ -296,6 +313,9 @@ k_conv3d_fwd_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__rest
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
   const uint32_t sxa = smem_u32(sx), swa = smem_u32(swt);
+  float bv[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) bv[k] = bias ? bias[k] : 0.f;
   const int ntx = (W + kTcX - 1) / kTcX, nty = (H + kTcY - 1) / kTcY;
   const long long ntiles = (long long)ntx * nty * D;
   int phase = 0;
@@ -320,14 +340,7 @@ k_conv3d_fwd_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__rest
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll 1
-      for (int t = 0; t < 27; ++t) {
-        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-        const uint32_t a = sxa + (uint32_t)(((dz * kTcSY + dy) * kTcSX + dx) * 16);
-        const uint64_t ad = tc_desc(a, kTcPlane, kTcSX * 16);
-        const uint64_t bd = tc_desc(swa + (uint32_t)(t * 2 * kC * 16), kC * 16, 8 * 16);
-        tc_mma(tmem, ad, bd, t > 0 ? 1u : 0u);
-      }
+      tc_tile_mmas(tmem, sxa, kTcPlane, swa);
       tc_commit(&bar);
     }
     // every thread decides on the same value: tcgen05.ld is warp-collective
@@ -344,7 +357,7 @@ k_conv3d_fwd_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__rest
         float o[16];
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
-          o[k] = v[k] + (bias ? bias[k] : 0.f);
+          o[k] = v[k] + bv[k];
           if (relu) o[k] = fmaxf(o[k], 0.f);
         }
         if (yb) {
@@ -382,16 +395,19 @@ k_conv3d_fwd_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__rest
 // The same tile and MMAs with the input staged by bulk tensor copies and
 // the work software-pipelined: while the warps drain tile j's accumulator,
 // the tensor cores already work on tile j+1 (two accumulators of 16 TMEM
-// columns, used in turn) and the copy engine fills a third stage with tile
-// j+2.  The tensor map views x as [D][H][W][2 halves][8 channels]; a box of
-// 8 x 1 x 10 x 18 x 3 is one channel-half plane of the staged tile in exactly
-// the layout above (zeros outside the volume), so each stage takes two
-// copies.  Half planes start 128-byte aligned.
+// columns, used in turn) and the copy engine fills stages ahead.  With NS
+// stages the copies of tile j+NS-1 are issued as soon as their stage is
+// free: for NS = 3 right after tile j+1's MMAs (the stage last held tile
+// j-1, whose MMAs completed in the previous iteration), for NS = 2 once tile
+// j's MMAs completed.  The tensor map views x as [D][H][W][2 halves][8
+// channels]; a box of 8 x 1 x 10 x 18 x 3 is one channel-half plane of the
+// staged tile in exactly the layout above (zeros outside the volume), so
+// each stage takes two copies.  Half planes start 128-byte aligned.
 constexpr int kTc2Plane = (kTcPlane + 127) / 128 * 128;  // 8704
 constexpr int kTc2Stage = 2 * kTc2Plane;
-constexpr int kTc2Stages = 3;
 constexpr int kTc2Copy = 2 * kTcPlane;  // bytes the two copies deliver
-constexpr int kTc2Smem = kTc2Stages * kTc2Stage + kTcWBytes + 128;  // + alignment slack
+template <int NS>
+constexpr int tc2_smem() { return NS * kTc2Stage + kTcWBytes + 128; }  // + alignment slack
 
 __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, uint64_t *bar,
                                             int c0, int c1, int c2, int c3, int c4) {
@@ -403,17 +419,19 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+template <int NS>
 __global__ void __launch_bounds__(128)
 k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *__restrict__ w,
                  const float *__restrict__ bias, int D, int H, int W, int relu,
                  __nv_bfloat16 *__restrict__ yb, float *__restrict__ yf) {
+  static_assert(NS == 2 || NS == 3, "two or three stages");
   extern __shared__ unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full[kTc2Stages];  // stage filled (copies landed)
-  __shared__ __align__(8) uint64_t done[2];           // accumulator b complete
+  __shared__ __align__(8) uint64_t full[NS];  // stage filled (copies landed)
+  __shared__ __align__(8) uint64_t done[2];   // accumulator b complete
   __shared__ uint32_t tmem_slot;
   __shared__ int s_abort;
   unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  unsigned char *swt = smem + kTc2Stages * kTc2Stage;  // [t][half][co] x 16 B
+  unsigned char *swt = smem + NS * kTc2Stage;  // [t][half][co] x 16 B
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntx = (W + kTcX - 1) / kTcX, nty = (H + kTcY - 1) / kTcY;
   const long long ntiles = (long long)ntx * nty * D;
@@ -429,11 +447,11 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
   };
   const uint32_t swa = smem_u32(swt);
   uint32_t tmem = 0;
-  // thread 0: copies of tile j into stage j % 3
+  // thread 0: copies of tile j into stage j % NS
   auto issue = [&](long long j) {
     int x0, y0, z;
     tile_origin(j, x0, y0, z);
-    const int s = (int)(j % kTc2Stages);
+    const int s = (int)(j % NS);
     mbar_arrive_expect_tx(&full[s], kTc2Copy);
     unsigned char *dst = smem + s * kTc2Stage;
     tma_load_5d(dst, &xmap, &full[s], 0, 0, x0 - 1, y0 - 1, z - 1);
@@ -441,25 +459,16 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
   };
   // thread 0: the 27 MMAs of tile j into accumulator j & 1, once its stage landed
   auto mma = [&](long long j) -> bool {
-    const int s = (int)(j % kTc2Stages);
-    if (!mbar_wait_bounded(&full[s], (uint32_t)((j / kTc2Stages) & 1))) return false;
+    const int s = (int)(j % NS);
+    if (!mbar_wait_bounded(&full[s], (uint32_t)((j / NS) & 1))) return false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t sxa = smem_u32(smem + s * kTc2Stage);
-    const uint32_t d = tmem + (uint32_t)((j & 1) * kC);
-#pragma unroll 1
-    for (int t = 0; t < 27; ++t) {
-      const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-      const uint32_t a = sxa + (uint32_t)(((dz * kTcSY + dy) * kTcSX + dx) * 16);
-      const uint64_t ad = tc_desc(a, kTc2Plane, kTcSX * 16);
-      const uint64_t bd = tc_desc(swa + (uint32_t)(t * 2 * kC * 16), kC * 16, 8 * 16);
-      tc_mma(d, ad, bd, t > 0 ? 1u : 0u);
-    }
+    tc_tile_mmas(tmem + (uint32_t)((j & 1) * kC), smem_u32(smem + s * kTc2Stage), kTc2Plane, swa);
     tc_commit(&done[j & 1]);
     return true;
   };
   long long n_tma = 0, n_mma = 0;  // thread 0: tiles whose copies / MMAs were issued
   if (tid == 0) {
-    for (int s = 0; s < kTc2Stages; ++s) mbar_init(&full[s], 1);
+    for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
     mbar_init(&done[0], 1);
     mbar_init(&done[1], 1);
     fence_mbar_init();
@@ -471,6 +480,9 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
     *reinterpret_cast<uint4 *>(swt + ((t * 2 + h) * kC + co) * 16) =
         *reinterpret_cast<const uint4 *>(w + (t * kC + co) * kC + h * 8);
   }
+  float bv[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) bv[q] = bias ? bias[q] : 0.f;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(
                      smem_u32(&tmem_slot))
@@ -490,13 +502,12 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
   bool ok = !s_abort;
   for (long long j = 0; j < nj && ok; ++j) {
     if (tid == 0 && !s_abort) {
-      // accumulator (j+1)&1 was drained in iteration j-1; stage (j+2)%3 was
-      // last read by tile j-1's MMAs, which completed before that drain
+      // accumulator (j+1)&1 was drained in iteration j-1
       if (j + 1 < nj) {
         if (mma(j + 1)) n_mma = j + 2;
         else s_abort = 1;
       }
-      if (!s_abort && j + 2 < nj) {
+      if (NS == 3 && !s_abort && j + 2 < nj) {
         issue(j + 2);
         n_tma = j + 3;
       }
@@ -504,6 +515,10 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
     // every thread takes the same branch: tcgen05.ld is warp-collective
     const bool got =
         __syncthreads_and(mbar_wait_bounded(&done[j & 1], (uint32_t)((j >> 1) & 1)));
+    if (NS == 2 && tid == 0 && got && !s_abort && j + 2 < nj) {
+      issue(j + 2);  // stage j % 2: tile j's MMAs completed
+      n_tma = j + 3;
+    }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (got) {
       int x0, y0, z;
@@ -517,7 +532,7 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
         float o[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
-          o[q] = v[q] + (bias ? bias[q] : 0.f);
+          o[q] = v[q] + bv[q];
           if (relu) o[q] = fmaxf(o[q], 0.f);
         }
         if (yb) {
@@ -548,7 +563,7 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
     // bounded waits for what may still be in flight: the copies of tiles
     // whose MMAs were never issued, and the last MMAs issued
     for (long long j = n_mma; j < n_tma; ++j)
-      mbar_wait_bounded(&full[j % kTc2Stages], (uint32_t)((j / kTc2Stages) & 1));
+      mbar_wait_bounded(&full[j % NS], (uint32_t)((j / NS) & 1));
     if (n_mma > 0) mbar_wait_bounded(&done[(n_mma - 1) & 1], (uint32_t)(((n_mma - 1) >> 1) & 1));
   }
   __syncthreads();
@@ -562,10 +577,10 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
 using namespace efwi;
 
 namespace {
-// 0: mma.sync; 1: tcgen05, tile staged by loads; 2: tcgen05, tiles staged by
-// bulk tensor copies two stages deep
+// 0: mma.sync; 1: tcgen05, tile staged by loads; 2 / 3: tcgen05, tiles
+// staged by bulk tensor copies two / three stages deep
 std::atomic<int> g_conv_kernel{2};
-std::atomic<unsigned long long> g_tc_smem_set{0}, g_tc2_smem_set{0};
+std::atomic<unsigned long long> g_tc_smem_set{0}, g_tc2_smem_set{0}, g_tc3_smem_set{0};
 int g_sm_count[64] = {0};
 std::atomic<PFN_cuTensorMapEncodeTiled_v12000> g_conv_encode{nullptr};
 
@@ -599,7 +614,7 @@ bool conv_map(CUtensorMap *m, const void *x, int D, int H, int W) {
 }  // namespace
 
 extern "C" int efwi_conv3d_set_kernel(int form) {
-  if (form < 0 || form > 2) return 1;
+  if (form < 0 || form > 3) return 1;
   g_conv_kernel.store(form);
   return 0;
 }
@@ -632,13 +647,20 @@ extern "C" int efwi_conv3d_forward(const void *x, const void *w, const float *bi
     if (!sms && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       return 2;
     const long long tiles = (long long)((W + kTcX - 1) / kTcX) * ((H + kTcY - 1) / kTcY) * D;
-    if (form == 2) {
+    if (form >= 2) {
       CUtensorMap map;
       if (!conv_map(&map, x, D, H, W)) return 2;
-      set_smem_once(k_conv3d_fwd_tc2, kTc2Smem, g_tc2_smem_set);
-      const int blocks = (int)std::min<long long>(tiles, 3LL * sms);  // 66 KB of shared memory each
-      k_conv3d_fwd_tc2<<<blocks, 128, kTc2Smem, st>>>(map, (const __nv_bfloat16 *)w, bias, D, H,
-                                                      W, relu, (__nv_bfloat16 *)y_bf16, y_f32);
+      if (form == 2) {  // two stages, 49 KB of shared memory: 4 CTAs per SM
+        set_smem_once(k_conv3d_fwd_tc2<2>, tc2_smem<2>(), g_tc2_smem_set);
+        const int blocks = (int)std::min<long long>(tiles, 4LL * sms);
+        k_conv3d_fwd_tc2<2><<<blocks, 128, tc2_smem<2>(), st>>>(
+            map, (const __nv_bfloat16 *)w, bias, D, H, W, relu, (__nv_bfloat16 *)y_bf16, y_f32);
+      } else {  // three stages, 66 KB: 3 CTAs per SM
+        set_smem_once(k_conv3d_fwd_tc2<3>, tc2_smem<3>(), g_tc3_smem_set);
+        const int blocks = (int)std::min<long long>(tiles, 3LL * sms);
+        k_conv3d_fwd_tc2<3><<<blocks, 128, tc2_smem<3>(), st>>>(
+            map, (const __nv_bfloat16 *)w, bias, D, H, W, relu, (__nv_bfloat16 *)y_bf16, y_f32);
+      }
     } else {
       set_smem_once(k_conv3d_fwd_tc, kTcSmem, g_tc_smem_set);
       const int blocks = (int)std::min<long long>(tiles, 6LL * sms);
