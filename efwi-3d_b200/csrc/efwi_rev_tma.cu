@@ -213,7 +213,8 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
             basxx{ring.halo(q, L::HA + 2) + off}, basxy{ring.halo(q, L::HA + 3) + off},
             basyy{ring.halo(q, L::HA + 4) + off}, baszz{ring.halo(q, L::HA + 5) + off};
         const bool zs = slab_s(z, nz, np);
-        const Coef cz = coef(g.cz, nz, z);
+        // outside the z slab the profile is K = 1, a = 0 (b unused there)
+        const Coef cz = zs ? coef(g.cz, nz, z) : Coef{1.f, 0.f, 0.f, 1.f, 0.f, 0.f};
         const float l = ring.point(q, L::ML)[pt], u = ring.point(q, L::MM)[pt], l2u = l + 2.0f * u;
         float nax, naz, nay;  // the new adjoint velocities (before res_injection)
         {  // adjoint vx
@@ -419,7 +420,8 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
       }
       if (do_adj) {
         const bool zs = slab_s(z, nz, np);
-        const Coef cz = coef(g.cz, nz, z);
+        // outside the z slab the profile is K = 1, a = 0 (b unused there)
+        const Coef cz = zs ? coef(g.cz, nz, z) : Coef{1.f, 0.f, 0.f, 1.f, 0.f, 0.f};
         const float b = ring.point(q, 14)[pt];
         {  // sxz
           const float dvz_dx = -dplus(bavz.x(-1), avz.c, bavz.x(1), bavz.x(2)) * idx;
