@@ -202,8 +202,19 @@ def make_pairs(n_pairs: int = 200, n: int = 40, nt: int = 500, nprobe: int = 4, 
     return out
 
 
+def _cosine_loss(pred: torch.Tensor, y: torch.Tensor) -> torch.Tensor:
+    """1 - cos(pred, y) over the whole volume: only the direction counts (the
+    L-BFGS recursion rescales the map's output), and every cell weighs by its
+    share of the norm rather than by its size relative to the largest entry
+    (a mean squared error of max-normalised directions is near its floor
+    for any output close to zero)."""
+    p, t = pred.reshape(-1), y.reshape(-1)
+    return 1.0 - torch.dot(p, t) / (torch.linalg.vector_norm(p) * torch.linalg.vector_norm(t) + 1e-30)
+
+
 def train(net, pairs, epochs: int = 20, lr: float = 2e-3, seed: int = 0, log=None) -> List[float]:
-    """Adam on the mean squared error of the normalised direction."""
+    """Adam on one minus the cosine between the network's output and the
+    target direction."""
     opt = torch.optim.Adam(net.parameters(), lr=lr)
     g = torch.Generator().manual_seed(seed)
     hist = []
@@ -213,7 +224,7 @@ def train(net, pairs, epochs: int = 20, lr: float = 2e-3, seed: int = 0, log=Non
         for i in order:
             opt.zero_grad()
             pred = net(pairs[i]["x"])
-            loss = torch.mean((pred - pairs[i]["y"]) ** 2)
+            loss = _cosine_loss(pred, pairs[i]["y"])
             loss.backward()
             opt.step()
             tot += loss.item()

@@ -109,3 +109,16 @@ def test_lbfgs_steps_on_gradients_whose_squares_underflow_fp32():
     res = lbfgs(obj, torch.full_like(obj.vp_true, 2500.0), iters=6)
     assert len(res.misfit) == 7
     assert res.misfit[-1] < 0.5 * res.misfit[0]
+
+
+def test_training_loss_sees_direction_only():
+    import torch
+    from efwi.preconditioner import _cosine_loss
+    g = torch.Generator().manual_seed(1)
+    a = torch.randn(3, 4, 5, generator=g, dtype=torch.float64)
+    assert abs(float(_cosine_loss(3.0 * a, a))) < 1e-12
+    assert abs(float(_cosine_loss(-a, a)) - 2.0) < 1e-12
+    p = torch.randn(3, 4, 5, generator=g, dtype=torch.float64, requires_grad=True)
+    _cosine_loss(p, a).backward()
+    # the loss does not change along p itself: its gradient is orthogonal to p
+    assert abs(float(torch.sum(p.grad * p))) < 1e-10
