@@ -378,6 +378,7 @@ def lbfgs(obj: VpObjective, vp0: torch.Tensor, iters: int = 20, memory: int = 10
                 f"model rel-L2 {res.model_rel_l2[-1]:.4e}")
         if stop_misfit is not None and J <= stop_misfit:
             break
+    res.evals = obj.evals  # trial points of a failed last search included
     return res
 
 
