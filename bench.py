@@ -762,6 +762,8 @@ def main():
             F.fwi_ops.backward(lam_h, mu_h, rho_h, stf_h, 1, sid, para)  # loads obs into HBM
             torch.cuda.synchronize()
             f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            clk_e2e = Clocks(local)  # sampled as in the device-timed region
+            clk_e2e.start()
             f0.record(stream)
             for _ in range(a.steps):
                 out = F.fwi_ops.backward(lam_h, mu_h, rho_h, stf_h, 1, sid, para)
@@ -771,6 +773,7 @@ def main():
                     _ = gsum.cpu()
             f1.record(stream)
             torch.cuda.synchronize()
+            clocks_e2e = clk_e2e.stop()
             ms_e2e = f0.elapsed_time(f1) / a.steps
             if world > 1:
                 t = torch.tensor([ms_e2e], device=dev)
@@ -779,7 +782,8 @@ def main():
             nb = g.ncell * 4
             e2e = {"value": cells_step / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
                    "h2d_bytes_per_step": 3 * nb, "d2h_bytes_per_step": 3 * nb + 4,
-                   "ms_per_step": ms_e2e, "api": "FWI_ops_3d.fwi_ops.backward (host tensors)"}
+                   "ms_per_step": ms_e2e, "api": "FWI_ops_3d.fwi_ops.backward (host tensors)",
+                   "clocks": clocks_e2e}
 
     parity = None
     if rank == 0 and world == 1 and not a.no_cpu and a.parity_nt > 0:
