@@ -235,14 +235,22 @@ def test_exact_tile_width_is_bitwise_neutral():
 
 
 def test_adjoint_of_the_residual_is_the_exact_gradient():
-    """J^T w with w = dJ/dsyn = -2 res gives the exact gradient (bitwise)."""
+    """J^T w with w = dJ/dsyn = -2 res gives the exact gradient: bitwise on
+    one lane (the same per-shot sums in the same order); with two shot lanes
+    the gradient adds the lanes' images in lane order, 1e-6."""
     p = _problem(nshot=2)
     obs = _obs(p)
     P = _engine(p)
+    P.set_lanes(1)
     J, gl, gm, gr, res = P.gradient([0, 1], obs, mode="exact", want_residual=True)
     al, am, ar = P.adjoint([0, 1], -2.0 * res)
     for a, b in ((al, gl), (am, gm), (ar, gr)):
         assert torch.equal(a, b)
+    P.set_lanes(2)
+    J2, gl2, gm2, gr2 = P.gradient([0, 1], obs, mode="exact")
+    assert J2 == J
+    for a, b in ((al, gl2), (am, gm2), (ar, gr2)):
+        assert rel_l2(a.cpu(), b.cpu()) < 1e-6
 
 
 def test_illumination_matches_oracle():
