@@ -556,7 +556,7 @@ def run_cnn(a):
     x = torch.randn(a.n, a.n, a.n, 16, device="cuda", generator=g).to(torch.bfloat16)
     w = (0.2 * torch.randn(27, 16, 16, device="cuda", generator=g)).to(torch.bfloat16)
     forms = {}
-    for form in ("mma", "tcgen05", "tcgen05-tma", "tcgen05-tma3"):
+    for form in ("mma", "tcgen05", "tcgen05-tma", "tcgen05-tma3", "tcgen05-ws", "tcgen05-ws3"):
         set_conv_kernel(form)
         for _ in range(3):
             conv3d_raw(x, w, None, True)

@@ -571,6 +571,181 @@ k_conv3d_fwd_tc2(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
 }
 
+
+// Warp-specialised form of the copy-staged kernel: warp 0 (one elected
+// thread) fills NS stages with bulk tensor copies and issues each tile's 27
+// MMAs into one of two accumulators; warps 1-4 drain the accumulators
+// (warp w reads TMEM lanes 32 (w % 4) .. + 31, so the four cover the 128
+// rows).  The roles meet only at mbarriers -- stage full (copies landed),
+// stage empty (its MMAs completed, committed by the MMA thread), accumulator
+// full (committed) and accumulator empty (one arrival per epilogue warp
+// after its tcgen05.ld) -- so no warp waits for the CTA at a barrier per
+// tile.  Every wait is bounded: a role that gives up sets the status flag
+// and a shared abort word that the other roles test once per tile; before
+// TMEM is freed, thread 0 waits (bounded) for the copies and MMAs it issued.
+constexpr int kWsThreads = 160;
+
+__device__ __forceinline__ void mbar_arrive1(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <int NS>
+__global__ void __launch_bounds__(kWsThreads)
+k_conv3d_fwd_ws(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *__restrict__ w,
+                const float *__restrict__ bias, int D, int H, int W, int relu,
+                __nv_bfloat16 *__restrict__ yb, float *__restrict__ yf) {
+  static_assert(NS >= 2 && NS <= 4, "two to four stages");
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full[NS], empty[NS], tfull[2], tempty[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int s_abort;
+  unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  unsigned char *swt = smem + NS * kTc2Stage;  // [t][half][co] x 16 B
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntx = (W + kTcX - 1) / kTcX, nty = (H + kTcY - 1) / kTcY;
+  const long long ntiles = (long long)ntx * nty * D;
+  const long long nj =
+      (long long)blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto tile_origin = [&](long long j, int &x0, int &y0, int &z) {
+    const long long tile = blockIdx.x + j * gridDim.x;
+    x0 = (int)(tile % ntx) * kTcX;
+    const long long r = tile / ntx;
+    y0 = (int)(r % nty) * kTcY;
+    z = (int)(r / nty);
+  };
+  auto give_up = [&]() {
+    s_abort = 1;
+    atomicExch(&g_conv_status, EFWI_STATUS_TIMEOUT);
+  };
+  auto issue = [&](long long j) {  // thread 0: copies of tile j into stage j % NS
+    int x0, y0, z;
+    tile_origin(j, x0, y0, z);
+    const int s = (int)(j % NS);
+    mbar_arrive_expect_tx(&full[s], kTc2Copy);
+    unsigned char *dst = smem + s * kTc2Stage;
+    tma_load_5d(dst, &xmap, &full[s], 0, 0, x0 - 1, y0 - 1, z - 1);
+    tma_load_5d(dst + kTc2Plane, &xmap, &full[s], 0, 1, x0 - 1, y0 - 1, z - 1);
+  };
+  long long jt = 0, jm = 0;  // thread 0: tiles whose copies / MMAs were issued
+  if (tid == 0) {
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    fence_mbar_init();
+    s_abort = 0;
+    for (; jt < NS && jt < nj; ++jt) issue(jt);
+  }
+  for (int k = tid; k < 27 * 2 * kC; k += blockDim.x) {
+    const int t = k / (2 * kC), r = k % (2 * kC), h = r / kC, co = r % kC;
+    *reinterpret_cast<uint4 *>(swt + ((t * 2 + h) * kC + co) * 16) =
+        *reinterpret_cast<const uint4 *>(w + (t * kC + co) * kC + h * 8);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(
+                     smem_u32(&tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async_smem();  // the staged weights are read by the tensor cores
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t swa = smem_u32(swt);
+
+  if (warp == 0) {
+    if (lane == 0) {  // copies and MMAs
+      for (long long j = 0; j < nj; ++j) {
+        if (s_abort) break;
+        const int s = (int)(j % NS), b = (int)(j & 1);
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((j / NS) & 1))) { give_up(); break; }
+        if (j >= 2 && !mbar_wait_bounded(&tempty[b], (uint32_t)(((j - 2) >> 1) & 1))) {
+          give_up();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        tc_tile_mmas(tmem + (uint32_t)(b * kC), smem_u32(smem + s * kTc2Stage), kTc2Plane, swa);
+        tc_commit(&tfull[b]);
+        tc_commit(&empty[s]);
+        jm = j + 1;
+        // refill the stage of tile j-1 (its MMAs were issued one tile ago)
+        if (j >= 1 && jt < nj) {
+          const long long jp = j - 1;
+          if (!mbar_wait_bounded(&empty[jp % NS], (uint32_t)((jp / NS) & 1))) { give_up(); break; }
+          issue(jt);
+          ++jt;
+        }
+      }
+    }
+  } else if (warp <= 4) {  // epilogue: TMEM lanes 32 (warp % 4) .. + 31
+    const int q = warp & 3;
+    float bv[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) bv[k] = bias ? bias[k] : 0.f;
+    for (long long j = 0; j < nj; ++j) {
+      if (s_abort) break;
+      const int b = (int)(j & 1);
+      bool ok = mbar_wait_bounded(&tfull[b], (uint32_t)((j >> 1) & 1));
+      ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
+      if (!ok) {
+        if (lane == 0) give_up();
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      float v[16];
+      tc_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kC), v);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive1(&tempty[b]);
+      int x0, y0, z;
+      tile_origin(j, x0, y0, z);
+      const int m = q * 32 + lane;
+      const int xv = x0 + (m & 7), yv = y0 + (m >> 3);
+      if (xv < W && yv < H) {
+        const long long off = (((long long)z * H + yv) * W + xv) * kC;
+        float o[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          o[k] = v[k] + bv[k];
+          if (relu) o[k] = fmaxf(o[k], 0.f);
+        }
+        if (yb) {
+          uint32_t pk[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(o[2 * k], o[2 * k + 1]);
+            pk[k] = *reinterpret_cast<const uint32_t *>(&b2);
+          }
+          uint4 *dst = reinterpret_cast<uint4 *>(yb + off);
+          dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        }
+        if (yf) {
+          float4 *dst = reinterpret_cast<float4 *>(yf + off);
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            dst[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    // bounded waits for what thread 0 issued and nobody consumed: copies of
+    // tiles whose MMAs were never issued, and the last MMAs (their commit)
+    for (long long j = jm; j < jt; ++j) mbar_wait_bounded(&full[j % NS], (uint32_t)((j / NS) & 1));
+    if (jm > 0) mbar_wait_bounded(&empty[(jm - 1) % NS], (uint32_t)(((jm - 1) / NS) & 1));
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+}
 }  // namespace
 }  // namespace efwi
 
@@ -578,9 +753,11 @@ using namespace efwi;
 
 namespace {
 // 0: mma.sync; 1: tcgen05, tile staged by loads; 2 / 3: tcgen05, tiles
-// staged by bulk tensor copies two / three stages deep
+// staged by bulk tensor copies two / three stages deep; 4 / 5: the same,
+// warp-specialised (copy + MMA warp, four epilogue warps), two / three stages
 std::atomic<int> g_conv_kernel{2};
-std::atomic<unsigned long long> g_tc_smem_set{0}, g_tc2_smem_set{0}, g_tc3_smem_set{0};
+std::atomic<unsigned long long> g_tc_smem_set{0}, g_tc2_smem_set{0}, g_tc3_smem_set{0},
+    g_ws2_smem_set{0}, g_ws3_smem_set{0};
 int g_sm_count[64] = {0};
 std::atomic<PFN_cuTensorMapEncodeTiled_v12000> g_conv_encode{nullptr};
 
@@ -614,7 +791,7 @@ bool conv_map(CUtensorMap *m, const void *x, int D, int H, int W) {
 }  // namespace
 
 extern "C" int efwi_conv3d_set_kernel(int form) {
-  if (form < 0 || form > 3) return 1;
+  if (form < 0 || form > 5) return 1;
   g_conv_kernel.store(form);
   return 0;
 }
@@ -650,7 +827,20 @@ extern "C" int efwi_conv3d_forward(const void *x, const void *w, const float *bi
     if (form >= 2) {
       CUtensorMap map;
       if (!conv_map(&map, x, D, H, W)) return 2;
-      if (form == 2) {  // two stages, 49 KB of shared memory: 4 CTAs per SM
+      if (form >= 4) {  // warp-specialised: two stages at 4 CTAs per SM, or three at 3
+        const __nv_bfloat16 *wb = (const __nv_bfloat16 *)w;
+        if (form == 4) {
+          set_smem_once(k_conv3d_fwd_ws<2>, tc2_smem<2>(), g_ws2_smem_set);
+          const int blocks = (int)std::min<long long>(tiles, 4LL * sms);
+          k_conv3d_fwd_ws<2><<<blocks, kWsThreads, tc2_smem<2>(), st>>>(
+              map, wb, bias, D, H, W, relu, (__nv_bfloat16 *)y_bf16, y_f32);
+        } else {
+          set_smem_once(k_conv3d_fwd_ws<3>, tc2_smem<3>(), g_ws3_smem_set);
+          const int blocks = (int)std::min<long long>(tiles, 3LL * sms);
+          k_conv3d_fwd_ws<3><<<blocks, kWsThreads, tc2_smem<3>(), st>>>(
+              map, wb, bias, D, H, W, relu, (__nv_bfloat16 *)y_bf16, y_f32);
+        }
+      } else if (form == 2) {  // two stages, 49 KB of shared memory: 4 CTAs per SM
         set_smem_once(k_conv3d_fwd_tc2<2>, tc2_smem<2>(), g_tc2_smem_set);
         const int blocks = (int)std::min<long long>(tiles, 4LL * sms);
         k_conv3d_fwd_tc2<2><<<blocks, 128, tc2_smem<2>(), st>>>(

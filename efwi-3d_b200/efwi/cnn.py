@@ -43,7 +43,8 @@ def conv3d_raw(x: torch.Tensor, wb: torch.Tensor, bias, relu: bool, out_f32: boo
     return yf if out_f32 else yb
 
 
-CONV_FORMS = {"mma": 0, "tcgen05": 1, "tcgen05-tma": 2, "tcgen05-tma3": 3}
+CONV_FORMS = {"mma": 0, "tcgen05": 1, "tcgen05-tma": 2, "tcgen05-tma3": 3, "tcgen05-ws": 4,
+              "tcgen05-ws3": 5}
 
 
 def set_conv_kernel(form: str) -> None:
@@ -51,8 +52,11 @@ def set_conv_kernel(form: str) -> None:
     process: 'mma' (mma.sync m16n8k16), 'tcgen05' (tensor-memory accumulator,
     one MMA per tap for 128 voxels, tile staged by loads), 'tcgen05-tma'
     (the same MMAs, tiles staged by bulk tensor copies two stages deep, the
-    next tile's MMAs overlapping this tile's epilogue; the default) or
-    'tcgen05-tma3' (three stages, fewer CTAs per SM)."""
+    next tile's MMAs overlapping this tile's epilogue; the default),
+    'tcgen05-tma3' (three stages, fewer CTAs per SM), 'tcgen05-ws' /
+    'tcgen05-ws3' (warp-specialised: one warp issues the copies and MMAs,
+    four drain the accumulators, mbarriers between them; two / three
+    stages)."""
     if form not in CONV_FORMS:
         raise ValueError(f"unknown convolution kernel form {form!r}")
     lib().efwi_conv3d_set_kernel(CONV_FORMS[form])

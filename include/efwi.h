@@ -279,7 +279,9 @@ int efwi_conv3d_wgrad(const void *x, const void *dy, int D, int H, int W, float 
  * 1 = tcgen05.mma with the accumulator in tensor memory (128 voxels x 16
  * channels per tile, one MMA per tap), tile staged by loads; 2 / 3 = the
  * same MMAs with the tiles staged by bulk tensor copies two / three stages
- * deep and the next tile's MMAs overlapping this tile's epilogue.  All
+ * deep and the next tile's MMAs overlapping this tile's epilogue; 4 / 5 =
+ * the same warp-specialised (one warp issues the copies and MMAs, four
+ * drain the accumulators; mbarriers between them), two / three stages.  All
  * give the same sums up to FP32 rounding order.  The tcgen05 forms need w
  * and the outputs 16-byte aligned and fall back to mma.sync otherwise.
  * Returns 1 for an unknown form.  efwi_conv3d_status reads and clears the

@@ -45,7 +45,8 @@ def test_forward_matches_torch(shape, relu):
     assert rel_l2(ours_b.float().cpu(), ref.cpu()) < 1e-2
 
 
-@pytest.mark.parametrize("form_tc", ["tcgen05", "tcgen05-tma", "tcgen05-tma3"])
+@pytest.mark.parametrize("form_tc", ["tcgen05", "tcgen05-tma", "tcgen05-tma3", "tcgen05-ws",
+                                     "tcgen05-ws3"])
 @pytest.mark.parametrize("shape", [(1, 1, 1), (3, 17, 9), (4, 33, 70), (2, 16, 8)])
 def test_tcgen05_form_matches_mma_form_and_torch(shape, form_tc):
     """The tcgen05 convolution (accumulator in tensor memory) against the
