@@ -68,9 +68,11 @@ def parse():
     ap.add_argument("--no-graphs", dest="graphs", action="store_false",
                     help="launch the time loops' kernels one by one instead of replaying "
                          "captured CUDA graphs (same kernels, same work)")
-    ap.add_argument("--mode", default="reference", choices=["reference", "exact"],
-                    help="gradient algorithm: the reference's (headline) or the exact "
-                         "discrete adjoint with binomial checkpoints")
+    ap.add_argument("--mode", default=None, choices=["reference", "exact"],
+                    help="gradient algorithm: the reference's (headline; the default) or the "
+                         "exact discrete adjoint with binomial checkpoints (the default of "
+                         "--case inversion: the line search accepts no step along the "
+                         "reference's approximate image there)")
     ap.add_argument("--ck-budget", type=float, default=16.0,
                     help="GiB of checkpoint slots of the exact gradient")
     ap.add_argument("--case", default=None,
@@ -81,14 +83,17 @@ def parse():
                          "cases, and the main run with --no-autotune)")
     ap.add_argument("--iters", type=int, default=20, help="inversion case: L-BFGS iterations")
     ap.add_argument("--pairs", type=int, default=200, help="inversion case: training pairs")
-    ap.add_argument("--pair-n", type=int, default=40, help="inversion case: model cells of a pair")
-    ap.add_argument("--pair-nt", type=int, default=500)
-    ap.add_argument("--nprobe", type=int, default=4)
-    ap.add_argument("--net-mode", default="step", choices=["step", "h0"],
+    ap.add_argument("--pair-n", type=int, default=64, help="inversion case: model cells of a pair")
+    ap.add_argument("--pair-nt", type=int, default=800)
+    ap.add_argument("--nprobe", type=int, default=2)
+    ap.add_argument("--net-mode", default="h0", choices=["step", "h0"],
                     help="inversion case: the CNN's direction tried first ('step') or the CNN "
                          "as the initial inverse Hessian of L-BFGS ('h0')")
     ap.add_argument("--epochs", type=int, default=20)
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.mode is None:
+        a.mode = "exact" if a.case == "inversion" else "reference"
+    return a
 
 
 def peaks():
