@@ -98,7 +98,7 @@ def test_config1_full_time_axis_well_conditioned_gradients():
 
 def test_config2_one_shot_full_grid():
     """Config 2's 152^3 padded grid, one shot at nt 500 (the full nt 2000
-    takes the host checkers about 20 minutes): traces of the true model,
+    takes the host checkers about 8 minutes: the opt-in test below): traces of the true model,
     misfit and reference gradient of the smoothed initial model against
     them, compared with the reference's kernels and the FP64 port."""
     from efwi import synthetic
@@ -121,6 +121,33 @@ def test_config2_one_shot_full_grid():
     assert abs(J - Jp) / Jp < 1e-4
     for a, b in zip(ours, port):
         assert rel_l2(a, b) < 1e-4
+
+
+@pytest.mark.skipif(not __import__("os").environ.get("EFWI_FULL_TIME_AXIS"),
+                    reason="about 8 minutes of host work; set EFWI_FULL_TIME_AXIS=1")
+def test_config2_one_shot_full_time_axis():
+    """Config 2's full time axis (nt 2000), one shot: misfit and reference
+    gradients against the reference's kernels and the FP64 port.  The
+    reference's time-reversed source wavefield is unstable over 2000 steps
+    (its image is four orders of magnitude larger than the exact gradient
+    there, in FP64 as well), which amplifies rounding: lambda and mu are
+    held to 1e-4 of both; rho, whose image the reference's own FP32 kernels
+    carry about 1e-4 from FP64, to no more than 3 times that distance."""
+    from efwi import synthetic
+    nt = 2000
+    p = synthetic.config2(nt=nt, nshot=1)
+    P = _engine(p, "true")
+    tr = P.forward([0]).cpu().numpy()
+    P.set_model(*[torch.from_numpy(x) for x in p.params("init")])
+    J, ours = _grads(P, [0], torch.from_numpy(tr))
+    P.close()
+    obs = tr.reshape(3, -1, nt)
+    Jr, *ref, _ = oracle.ref().gradient(case_of(p, "init", np.float32), [obs])
+    Jp, *port, _ = oracle.port().gradient(case_of(p), [obs.astype(np.float64)], mode=0)
+    assert abs(J - Jr) / Jr < 1e-5 and abs(J - Jp) / Jp < 1e-5
+    for k in range(2):
+        assert rel_l2(ours[k], ref[k]) < 1e-4 and rel_l2(ours[k], port[k]) < 1e-4
+    assert rel_l2(ours[2], port[2]) < 3 * max(rel_l2(ref[2], port[2]), 1e-4)
 
 
 def test_config3_dot_product_on_the_full_grid():
