@@ -250,8 +250,9 @@ def _sync(dev) -> None:
 
 
 def _dot(a: torch.Tensor, b: torch.Tensor) -> float:
-    """Inner product in FP64: misfit gradients of FP32 volumes can be small
-    enough (1e-20 and below per cell) that their squares underflow FP32."""
+    """Inner product in FP64, so that the recursion does not depend on the
+    scale of the misfit (squares of small FP32 gradient entries underflow
+    FP32, and sums over millions of cells lose digits)."""
     return float(torch.sum(a.double() * b.double()))
 
 

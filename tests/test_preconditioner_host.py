@@ -88,9 +88,9 @@ def test_net_mode_is_checked():
 
 
 class _TinyQuadratic(_Quadratic):
-    """The same objective in FP32 with the misfit scaled by 1e-27, about as small
-    as the misfit gradients of the elastic problem get per cell: squares of
-    the gradient entries underflow FP32."""
+    """The same objective in FP32 with the misfit scaled by 1e-27, so that
+    squares of the gradient entries underflow FP32: the L-BFGS recursion
+    must not depend on the scale of the misfit."""
 
     SCALE = 1e-27
 
