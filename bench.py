@@ -790,6 +790,11 @@ def main():
                    "ms_per_step": ms_e2e, "api": "FWI_ops_3d.fwi_ops.backward (host tensors)",
                    "clocks": clocks_e2e}
 
+    # the engine's workspace (shell stores or checkpoint slots, up to most of
+    # the device) is not needed past this point: free it for the parity sample
+    P.close()
+    torch.cuda.empty_cache()
+
     parity = None
     if rank == 0 and world == 1 and not a.no_cpu and a.parity_nt > 0:
         parity = parity_sample(a, dev)
