@@ -290,8 +290,8 @@ int efwi_conv3d_wgrad(const void *x, const void *dy, int D, int H, int W, float 
 int efwi_conv3d_set_kernel(int form);
 int efwi_conv3d_status(int *timed_out, void *stream);
 
-/* Per-kernel timing with CUDA events on the call's stream (every
- * `sample`-th time step; 0 disables).  efwi_profile_read fills, for each
+/* Per-kernel timing with CUDA events on the call's stream (the time steps
+ * it with it % sample == sample / 2; 0 disables).  efwi_profile_read fills, for each
  * kernel class k < n, the number of timed launches, their total time in
  * milliseconds and the total number of launches of the class, and resets
  * the counters.  Class names: efwi_kernel_name(k). */
