@@ -419,8 +419,9 @@ struct Timer {
   Timer(EfwiHandle *h_, int cls_, cudaStream_t s_, int it) : h(h_), cls(cls_), s(s_) {
     h->launches[cls]++;
     // steps it = s/2, s/2 + s, ...: the first and last steps of a sweep
-    // (it = 0 has no adjoint update) stay out of the sample when s > 1
-    on = h->prof_sample > 0 && (it % h->prof_sample == h->prof_sample / 2);
+    // (it = 0 has no adjoint update) stay out of the sample when s > 1;
+    // launches outside the time loop (it < 0) are always timed
+    on = h->prof_sample > 0 && (it < 0 || it % h->prof_sample == h->prof_sample / 2);
     if (on) { a = next_event(h); b = next_event(h); cudaEventRecord(a, s); }
   }
   ~Timer() {
@@ -845,7 +846,7 @@ int misfit_shot(EfwiHandle *h, const ShotHost &sh, const float *obs, const float
     m.obs_w = m.syn_w + ntr;
   }
   {
-    Timer t(h, K_MISFIT, st, 0);
+    Timer t(h, K_MISFIT, st, -1);
     k_misfit<<<grid, dim3(32, 8), 0, st>>>(m, obs, syn_tm, res_tm, h->partial.as<double>());
     k_reduce_sum<<<1, 256, 0, st>>>(h->partial.as<double>(), nb, jdev);
   }
@@ -965,12 +966,12 @@ int exact_shot(EfwiHandle *h, int id, const float *obs, double *jdev, float *res
         if (rc) return rc;
       }
     } else if (act.op == CK_STORE) {
-      Timer t(h, K_CHECKPOINT, st, 0);
+      Timer t(h, K_CHECKPOINT, st, -1);
       float *dst = ck + (long long)act.a * SF;
       CK_CUDA(h, cudaMemcpyAsync(dst, state, sizeof(float) * 9 * N, cudaMemcpyDeviceToDevice, st));
       CK_CUDA(h, cudaMemcpyAsync(dst + 9 * N, psi, sizeof(float) * P, cudaMemcpyDeviceToDevice, st));
     } else if (act.op == CK_RESTORE) {
-      Timer t(h, K_CHECKPOINT, st, 0);
+      Timer t(h, K_CHECKPOINT, st, -1);
       if (act.a < 0) {
         CK_CUDA(h, cudaMemsetAsync(state, 0, sizeof(float) * 9 * N, st));
         CK_CUDA(h, cudaMemsetAsync(psi, 0, sizeof(float) * P, st));
@@ -1447,7 +1448,7 @@ int efwi_forward(EfwiHandle *h, int n, const int *ids, float *traces, void *stre
     for (int s = 0; s < S; ++s) {
       const int nr = h->shots[ids[b0 + s]].nrec;
       if (nr > 0) {
-        Timer t(h, K_OTHER, st, 0);
+        Timer t(h, K_OTHER, st, -1);
         k_traces_to_cr_t<<<dim3((nt + 31) / 32, (nr + 31) / 32, 3), dim3(32, 8), 0, st>>>(
             h->traces_tm.as<float>() + toff, traces + out_off, nt, nr);
       }
