@@ -1209,11 +1209,9 @@ int efwi_create(const EfwiGrid *g, EfwiHandle **out) {
   if (!g || !out) return EFWI_ERR_ARG;
   *out = nullptr;
   EfwiHandle *h = new EfwiHandle();
-  // at least 2 cells between the two C-PML slabs of every axis: a cell's
-  // slab neighbours within the stencil's reach then lie on its own side
-  if (g->nz < 5 || g->nx < 5 || g->ny < 5 || g->nt < 2 || g->npml < 2 ||
-      2 * g->npml + 2 > g->nz || 2 * g->npml + 2 > g->nx || 2 * g->npml + 2 > g->ny ||
-      !(g->dt > 0) || !(g->dz > 0) || !(g->dx > 0) || !(g->dy > 0)) {
+  if (g->nz < 5 || g->nx < 5 || g->ny < 5 || g->nt < 2 || g->npml < 2 || 2 * g->npml > g->nz ||
+      2 * g->npml > g->nx || 2 * g->npml > g->ny || !(g->dt > 0) || !(g->dz > 0) ||
+      !(g->dx > 0) || !(g->dy > 0)) {
     int rc = fail(h, EFWI_ERR_ARG, "invalid grid nz=%d nx=%d ny=%d npml=%d nt=%d", g->nz, g->nx,
                   g->ny, g->npml, g->nt);
     *out = h;

@@ -26,32 +26,29 @@ namespace efwi {
 
 namespace {
 
-// Adjoint memory variables at a cell's neighbours -2 .. 2 along one axis
-// (zero outside the slab).  The addressing is worked out once per thread
-// and plane: `base` is the slab offset of the thread's own cell, neighbour
-// i + d sits d * stride further (adjacent cells on one side of the slab
-// have adjacent slab indices), and bit d + 2 of `mask` says whether
-// neighbour i + d lies in the slab.  Active cells are at least 2 cells from
-// the grid's faces, so all five neighbours exist.
-struct SlabAxis {
-  int base, stride;
-  unsigned mask;
-};
-__device__ __forceinline__ unsigned slab_mask(int i, int n, int np) {
-  unsigned m = 0;
-#pragma unroll
-  for (int d = -2; d <= 2; ++d) m |= slab_s(i + d, n, np) ? (1u << (d + 2)) : 0u;
-  return m;
+__device__ __forceinline__ float nxp(const Geo &g, const float *p, int z, int x, int y) {
+  return -dplus(psi_x_get(g, p, z, x - 1, y), psi_x_get(g, p, z, x, y),
+                psi_x_get(g, p, z, x + 1, y), psi_x_get(g, p, z, x + 2, y));
 }
-__device__ __forceinline__ float sget(const float *p, const SlabAxis &s, int d) {
-  return ((s.mask >> (d + 2)) & 1u) ? p[s.base + d * s.stride] : 0.0f;
+__device__ __forceinline__ float nxm(const Geo &g, const float *p, int z, int x, int y) {
+  return -dminus(psi_x_get(g, p, z, x - 2, y), psi_x_get(g, p, z, x - 1, y),
+                 psi_x_get(g, p, z, x, y), psi_x_get(g, p, z, x + 1, y));
 }
-// -D+ and -D- of the variable at the cell
-__device__ __forceinline__ float snp(const float *p, const SlabAxis &s) {
-  return -dplus(sget(p, s, -1), sget(p, s, 0), sget(p, s, 1), sget(p, s, 2));
+__device__ __forceinline__ float nyp(const Geo &g, const float *p, int z, int x, int y) {
+  return -dplus(psi_y_get(g, p, z, x, y - 1), psi_y_get(g, p, z, x, y),
+                psi_y_get(g, p, z, x, y + 1), psi_y_get(g, p, z, x, y + 2));
 }
-__device__ __forceinline__ float snm(const float *p, const SlabAxis &s) {
-  return -dminus(sget(p, s, -2), sget(p, s, -1), sget(p, s, 0), sget(p, s, 1));
+__device__ __forceinline__ float nym(const Geo &g, const float *p, int z, int x, int y) {
+  return -dminus(psi_y_get(g, p, z, x, y - 2), psi_y_get(g, p, z, x, y - 1),
+                 psi_y_get(g, p, z, x, y), psi_y_get(g, p, z, x, y + 1));
+}
+__device__ __forceinline__ float nzp(const Geo &g, const float *p, int z, int x, int y) {
+  return -dplus(psi_z_get(g, p, z - 1, x, y), psi_z_get(g, p, z, x, y),
+                psi_z_get(g, p, z + 1, x, y), psi_z_get(g, p, z + 2, x, y));
+}
+__device__ __forceinline__ float nzm(const Geo &g, const float *p, int z, int x, int y) {
+  return -dminus(psi_z_get(g, p, z - 2, x, y), psi_z_get(g, p, z - 1, x, y),
+                 psi_z_get(g, p, z, x, y), psi_z_get(g, p, z + 1, x, y));
 }
 
 struct Coef {
@@ -119,8 +116,6 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
   const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
   const bool xin = x >= np && x <= nx - 1 - np, yin = y >= np && y <= ny - 1 - np;
   const bool xs = slab_s(x, nx, np), ys = slab_s(y, ny, np);
-  const int cxs = slab_c(x, nx, np), cys = slab_c(y, ny, np);
-  const unsigned mxs = slab_mask(x, nx, np), mys = slab_mask(y, ny, np);
   Coef cx{1.f, 0.f, 0.f, 1.f, 0.f, 0.f}, cy = cx;
   if (act) { cx = coef(g.cx, nx, x); cy = coef(g.cy, ny, y); }
   const float *psz = ps.z, *psx = ps.x, *psy = ps.y;
@@ -218,9 +213,6 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
             basxx{ring.halo(q, L::HA + 2) + off}, basxy{ring.halo(q, L::HA + 3) + off},
             basyy{ring.halo(q, L::HA + 4) + off}, baszz{ring.halo(q, L::HA + 5) + off};
         const bool zs = slab_s(z, nz, np);
-        const SlabAxis sx_{(z * (2 * np) + cxs) * ny + y, ny, mxs},
-            sy_{(z * nx + x) * (2 * np) + cys, 1, mys},
-            sz_{(slab_c(z, nz, np) * nx + x) * ny + y, nx * ny, slab_mask(z, nz, np)};
         // outside the z slab the profile is K = 1, a = 0 (b unused there)
         const Coef cz = zs ? coef(g.cz, nz, z) : Coef{1.f, 0.f, 0.f, 1.f, 0.f, 0.f};
         const float l = ring.point(q, L::ML)[pt], u = ring.point(q, L::MM)[pt], l2u = l + 2.0f * u;
@@ -234,14 +226,14 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
           float acc = l2u * dsxx_dx * cx.K * dt + l * dszz_dx * cx.K * dt +
                       l * dsyy_dx * cx.K * dt + u * cz.Kh * dsxz_dz * dt +
                       u * cy.Kh * dsxy_dy * dt;
-          if (xs) acc += cx.a * (snp(psx + PSI_VA * g.slab_x, sx_) * idx);
-          if (zs) acc += cz.ah * (snm(psz + PSI_VB1 * g.slab_z, sz_) * idz);
-          if (ys) acc += cy.ah * (snm(psy + PSI_VB2 * g.slab_y, sy_) * idy);
+          if (xs) acc += cx.a * (nxp(g, psx + PSI_VA * g.slab_x, z, x, y) * idx);
+          if (zs) acc += cz.ah * (nzm(g, psz + PSI_VB1 * g.slab_z, z, x, y) * idz);
+          if (ys) acc += cy.ah * (nym(g, psy + PSI_VB2 * g.slab_y, z, x, y) * idy);
           const float v = avx0 + acc;
           nax = v;
-          if (xs) { const long long k = PSI_SAA * g.slab_x + sx_.base; px[k] = cx.bh * px[k] + b * v * dt; }
-          if (zs) { const long long k = PSI_SAB1 * g.slab_z + sz_.base; pz[k] = cz.b * pz[k] + b * v * dt; }
-          if (ys) { const long long k = PSI_SAB2 * g.slab_y + sy_.base; py[k] = cy.b * py[k] + b * v * dt; }
+          if (xs) { const long long k = PSI_SAA * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.bh * px[k] + b * v * dt; }
+          if (zs) { const long long k = PSI_SAB1 * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.b * pz[k] + b * v * dt; }
+          if (ys) { const long long k = PSI_SAB2 * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.b * py[k] + b * v * dt; }
         }
         {  // adjoint vz
           const float dszz_dz = -dplus(aszz.a, aszz.b, aszz.c, aszz.d) * idz;
@@ -252,14 +244,14 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
           float acc = l2u * dszz_dz * cz.K * dt + l * dsxx_dz * cz.K * dt +
                       l * dsyy_dz * cz.K * dt + u * cy.Kh * dsyz_dy * dt +
                       u * cx.Kh * dsxz_dx * dt;
-          if (zs) acc += cz.a * (snp(psz + PSI_VA * g.slab_z, sz_) * idz);
-          if (ys) acc += cy.ah * (snm(psy + PSI_VB1 * g.slab_y, sy_) * idy);
-          if (xs) acc += cx.ah * (snm(psx + PSI_VB1 * g.slab_x, sx_) * idx);
+          if (zs) acc += cz.a * (nzp(g, psz + PSI_VA * g.slab_z, z, x, y) * idz);
+          if (ys) acc += cy.ah * (nym(g, psy + PSI_VB1 * g.slab_y, z, x, y) * idy);
+          if (xs) acc += cx.ah * (nxm(g, psx + PSI_VB1 * g.slab_x, z, x, y) * idx);
           const float v = avz0 + acc;
           naz = v;
-          if (xs) { const long long k = PSI_SAB1 * g.slab_x + sx_.base; px[k] = cx.b * px[k] + b * v * dt; }
-          if (zs) { const long long k = PSI_SAA * g.slab_z + sz_.base; pz[k] = cz.bh * pz[k] + b * v * dt; }
-          if (ys) { const long long k = PSI_SAB1 * g.slab_y + sy_.base; py[k] = cy.b * py[k] + b * v * dt; }
+          if (xs) { const long long k = PSI_SAB1 * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.b * px[k] + b * v * dt; }
+          if (zs) { const long long k = PSI_SAA * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.bh * pz[k] + b * v * dt; }
+          if (ys) { const long long k = PSI_SAB1 * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.b * py[k] + b * v * dt; }
         }
         {  // adjoint vy
           const float dsyy_dy = -dplus(basyy.y(-1), asyy.b, basyy.y(1), basyy.y(2)) * idy;
@@ -270,14 +262,14 @@ k_rev_velocity_tma(const __grid_constant__ Maps<K1L<MODE>::N> maps, Geo g, Field
           float acc = l2u * dsyy_dy * cy.K * dt + l * dsxx_dy * cy.K * dt +
                       l * dszz_dy * cy.K * dt + u * cx.Kh * dsxy_dx * dt +
                       u * cz.Kh * dsyz_dz * dt;
-          if (ys) acc += cy.a * (snp(psy + PSI_VA * g.slab_y, sy_) * idy);
-          if (xs) acc += cx.ah * (snm(psx + PSI_VB2 * g.slab_x, sx_) * idx);
-          if (zs) acc += cz.ah * (snm(psz + PSI_VB2 * g.slab_z, sz_) * idz);
+          if (ys) acc += cy.a * (nyp(g, psy + PSI_VA * g.slab_y, z, x, y) * idy);
+          if (xs) acc += cx.ah * (nxm(g, psx + PSI_VB2 * g.slab_x, z, x, y) * idx);
+          if (zs) acc += cz.ah * (nzm(g, psz + PSI_VB2 * g.slab_z, z, x, y) * idz);
           const float v = avy0 + acc;
           nay = v;
-          if (xs) { const long long k = PSI_SAB2 * g.slab_x + sx_.base; px[k] = cx.b * px[k] + b * v * dt; }
-          if (zs) { const long long k = PSI_SAB2 * g.slab_z + sz_.base; pz[k] = cz.bh * pz[k] + b * v * dt; }
-          if (ys) { const long long k = PSI_SAA * g.slab_y + sy_.base; py[k] = cy.b * py[k] + b * v * dt; }
+          if (xs) { const long long k = PSI_SAB2 * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.b * px[k] + b * v * dt; }
+          if (zs) { const long long k = PSI_SAB2 * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.bh * pz[k] + b * v * dt; }
+          if (ys) { const long long k = PSI_SAA * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.b * py[k] + b * v * dt; }
         }
         if (rmap >= 0) {  // res_injection after the adjoint update
           const int ur = inj.a.map[(long long)rmap * inj.a.nxpy + x * g.sx + y];
@@ -330,8 +322,6 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
   const float dt = g.dt, idz = g.idz, idx = g.idx, idy = g.idy;
   const bool xin = x >= np && x <= nx - 1 - np, yin = y >= np && y <= ny - 1 - np;
   const bool xs = slab_s(x, nx, np), ys = slab_s(y, ny, np);
-  const int cxs = slab_c(x, nx, np), cys = slab_c(y, ny, np);
-  const unsigned mxs = slab_mask(x, nx, np), mys = slab_mask(y, ny, np);
   Coef cx{1.f, 0.f, 0.f, 1.f, 0.f, 0.f}, cy = cx;
   if (act) { cx = coef(g.cx, nx, x); cy = coef(g.cy, ny, y); }
   const long long src_cell = (do_rev && src.cell) ? src.cell[0] : -1;
@@ -430,9 +420,6 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
       }
       if (do_adj) {
         const bool zs = slab_s(z, nz, np);
-        const SlabAxis sx_{(z * (2 * np) + cxs) * ny + y, ny, mxs},
-            sy_{(z * nx + x) * (2 * np) + cys, 1, mys},
-            sz_{(slab_c(z, nz, np) * nx + x) * ny + y, nx * ny, slab_mask(z, nz, np)};
         // outside the z slab the profile is K = 1, a = 0 (b unused there)
         const Coef cz = zs ? coef(g.cz, nz, z) : Coef{1.f, 0.f, 0.f, 1.f, 0.f, 0.f};
         const float b = ring.point(q, 14)[pt];
@@ -440,34 +427,34 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
           const float dvz_dx = -dplus(bavz.x(-1), avz.c, bavz.x(1), bavz.x(2)) * idx;
           const float dvx_dz = -dplus(avx.a, avx.b, avx.c, avx.d) * idz;
           float acc = dvz_dx * cx.K * b * dt + dvx_dz * cz.K * b * dt;
-          if (xs) acc += cx.a * (snp(psx + PSI_SAB1 * g.slab_x, sx_) * idx);
-          if (zs) acc += cz.a * (snp(psz + PSI_SAB1 * g.slab_z, sz_) * idz);
+          if (xs) acc += cx.a * (nxp(g, psx + PSI_SAB1 * g.slab_x, z, x, y) * idx);
+          if (zs) acc += cz.a * (nzp(g, psz + PSI_SAB1 * g.slab_z, z, x, y) * idz);
           const float s = axz0 + acc;
           a.sxz[i] = s;
-          if (xs) { const long long k = PSI_VB1 * g.slab_x + sx_.base; px[k] = cx.bh * px[k] + s * u * dt; }
-          if (zs) { const long long k = PSI_VB1 * g.slab_z + sz_.base; pz[k] = cz.bh * pz[k] + s * u * dt; }
+          if (xs) { const long long k = PSI_VB1 * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.bh * px[k] + s * u * dt; }
+          if (zs) { const long long k = PSI_VB1 * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.bh * pz[k] + s * u * dt; }
         }
         {  // sxy
           const float dvy_dx = -dplus(bavy.x(-1), avy.b, bavy.x(1), bavy.x(2)) * idx;
           const float dvx_dy = -dplus(bavx.y(-1), avx.b, bavx.y(1), bavx.y(2)) * idy;
           float acc = dvy_dx * cx.K * b * dt + dvx_dy * cy.K * b * dt;
-          if (xs) acc += cx.a * (snp(psx + PSI_SAB2 * g.slab_x, sx_) * idx);
-          if (ys) acc += cy.a * (snp(psy + PSI_SAB2 * g.slab_y, sy_) * idy);
+          if (xs) acc += cx.a * (nxp(g, psx + PSI_SAB2 * g.slab_x, z, x, y) * idx);
+          if (ys) acc += cy.a * (nyp(g, psy + PSI_SAB2 * g.slab_y, z, x, y) * idy);
           const float s = axy0 + acc;
           a.sxy[i] = s;
-          if (ys) { const long long k = PSI_VB2 * g.slab_y + sy_.base; py[k] = cy.bh * py[k] + s * u * dt; }
-          if (xs) { const long long k = PSI_VB2 * g.slab_x + sx_.base; px[k] = cx.bh * px[k] + s * u * dt; }
+          if (ys) { const long long k = PSI_VB2 * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.bh * py[k] + s * u * dt; }
+          if (xs) { const long long k = PSI_VB2 * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.bh * px[k] + s * u * dt; }
         }
         {  // syz
           const float dvz_dy = -dplus(bavz.y(-1), avz.c, bavz.y(1), bavz.y(2)) * idy;
           const float dvy_dz = -dplus(avy.a, avy.b, avy.c, avy.d) * idz;
           float acc = dvz_dy * cy.K * b * dt + dvy_dz * cz.K * b * dt;
-          if (ys) acc += cy.a * (snp(psy + PSI_SAB1 * g.slab_y, sy_) * idy);
-          if (zs) acc += cz.a * (snp(psz + PSI_SAB2 * g.slab_z, sz_) * idz);
+          if (ys) acc += cy.a * (nyp(g, psy + PSI_SAB1 * g.slab_y, z, x, y) * idy);
+          if (zs) acc += cz.a * (nzp(g, psz + PSI_SAB2 * g.slab_z, z, x, y) * idz);
           const float s = ayz0 + acc;
           a.syz[i] = s;
-          if (ys) { const long long k = PSI_VB1 * g.slab_y + sy_.base; py[k] = cy.bh * py[k] + s * u * dt; }
-          if (zs) { const long long k = PSI_VB2 * g.slab_z + sz_.base; pz[k] = cz.bh * pz[k] + s * u * dt; }
+          if (ys) { const long long k = PSI_VB1 * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.bh * py[k] + s * u * dt; }
+          if (zs) { const long long k = PSI_VB2 * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.bh * pz[k] + s * u * dt; }
         }
         {  // normal stresses
           const float dvx_dx = -dminus(bavx.x(-2), bavx.x(-1), avx.b, bavx.x(1)) * idx;
@@ -476,13 +463,13 @@ k_rev_stress_tma(const __grid_constant__ Maps<23> maps, Geo g, Fields f, Fields 
           float sxx = axx0 + b * dvx_dx * cx.Kh * dt;
           float szz = azz0 + b * dvz_dz * cz.Kh * dt;
           float syy = ayy0 + b * dvy_dy * cy.Kh * dt;
-          if (xs) sxx += cx.ah * (snm(psx + PSI_SAA * g.slab_x, sx_) * idx);
-          if (zs) szz += cz.ah * (snm(psz + PSI_SAA * g.slab_z, sz_) * idz);
-          if (ys) syy += cy.ah * (snm(psy + PSI_SAA * g.slab_y, sy_) * idy);
+          if (xs) sxx += cx.ah * (nxm(g, psx + PSI_SAA * g.slab_x, z, x, y) * idx);
+          if (zs) szz += cz.ah * (nzm(g, psz + PSI_SAA * g.slab_z, z, x, y) * idz);
+          if (ys) syy += cy.ah * (nym(g, psy + PSI_SAA * g.slab_y, z, x, y) * idy);
           a.sxx[i] = sxx; a.szz[i] = szz; a.syy[i] = syy;
-          if (xs) { const long long k = PSI_VA * g.slab_x + sx_.base; px[k] = cx.b * px[k] + l * szz * dt + l2u * sxx * dt + l * syy * dt; }
-          if (zs) { const long long k = PSI_VA * g.slab_z + sz_.base; pz[k] = cz.b * pz[k] + l2u * szz * dt + l * sxx * dt + l * syy * dt; }
-          if (ys) { const long long k = PSI_VA * g.slab_y + sy_.base; py[k] = cy.b * py[k] + l * szz * dt + l * sxx * dt + l2u * syy * dt; }
+          if (xs) { const long long k = PSI_VA * g.slab_x + psi_x_idx(g, z, x, y); px[k] = cx.b * px[k] + l * szz * dt + l2u * sxx * dt + l * syy * dt; }
+          if (zs) { const long long k = PSI_VA * g.slab_z + psi_z_idx(g, z, x, y); pz[k] = cz.b * pz[k] + l2u * szz * dt + l * sxx * dt + l * syy * dt; }
+          if (ys) { const long long k = PSI_VA * g.slab_y + psi_y_idx(g, z, x, y); py[k] = cy.b * py[k] + l * szz * dt + l * sxx * dt + l2u * syy * dt; }
         }
       }
     }

@@ -58,9 +58,7 @@ typedef struct {
   float src_weight;                 /* windowed misfit only */
 } EfwiShot;
 
-/* Replaces: cufd set-up (libCUFD.cu:52-91) and Cpml (Cpml.cu:7-99).
- * Rejects (EFWI_ERR_ARG) grids with fewer than 5 cells or fewer than
- * 2 * npml + 2 cells on an axis, npml < 2 or nt < 2. */
+/* Replaces: cufd set-up (libCUFD.cu:52-91) and Cpml (Cpml.cu:7-99). */
 int efwi_create(const EfwiGrid *grid, EfwiHandle **out);
 void efwi_destroy(EfwiHandle *h);
 const char *efwi_last_error(const EfwiHandle *h);
