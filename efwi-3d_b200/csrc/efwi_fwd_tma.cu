@@ -19,8 +19,6 @@
 
 namespace efwi {
 
-constexpr int FWD_RING = 4;
-
 template <int TX, int R, int MINB>
 __global__ void __launch_bounds__(32 * TX, MINB)
 k_stress_fwd_tma(const __grid_constant__ Maps<11> maps, Geo g, Fields f, Psi ps, int zchunk,
