@@ -575,6 +575,22 @@ def run_cnn(a):
         forms[form] = {"layer_ms": ms, "tflops": fl1 / (ms * 1e-3) / 1e12,
                        "frac_bf16": fl1 / (ms * 1e-3) / 1e12 / peak,
                        "gbs": by1 / (ms * 1e-3) / 1e9, "frac_hbm": by1 / (ms * 1e-3) / 1e9 / hbm}
+    from efwi.cnn import conv3d_wgrad, set_wgrad_kernel
+    dyv = torch.randn(a.n, a.n, a.n, 16, device="cuda", generator=g).to(torch.bfloat16)
+    wgrad = {}
+    for form in ("mma", "tcgen05"):
+        set_wgrad_kernel(form)
+        for _ in range(3):
+            conv3d_wgrad(x, dyv)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            conv3d_wgrad(x, dyv)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        wgrad[form] = {"ms": ms, "tflops": fl1 / (ms * 1e-3) / 1e12}
+    set_wgrad_kernel("mma")
     if conv3d_status():
         raise RuntimeError("a tcgen05 convolution timed out waiting for its tensor cores")
     set_conv_kernel(a.conv_form)
@@ -601,7 +617,7 @@ def run_cnn(a):
     print(json.dumps({"case": "cnn", "grid": a.n, "layers": layers, "fwd_ms": fwd_ms,
                       "fwd_bwd_ms": all_ms, "fwd_tflops": fl / (fwd_ms * 1e-3) / 1e12,
                       "fwd_bwd_tflops": 3 * fl / (all_ms * 1e-3) / 1e12,
-                      "one_layer_bf16_relu": forms,
+                      "one_layer_bf16_relu": forms, "weight_gradient": wgrad,
                       "peak_bf16_tflops": peak, "peak_hbm_gbs": hbm,
                       "network_form": a.conv_form,
                       "note": "network: forward and input-gradient convolutions in the named "

@@ -746,6 +746,145 @@ k_conv3d_fwd_ws(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *_
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
 }
+// Weight gradient on tcgen05: dW[t][co][ci] = sum_u dy[u - off_t][co] x[u][ci]
+// (u = v + off_t).  A unit is 8 (x) x 16 (y) voxels u at one z; its K = 16
+// slices are two staged rows of 8 voxels.  B = x[u][ci] staged as
+// [row][ci][8 x] (256-byte row blocks: ci halves 128 B apart, the second K
+// row one block on).  A stacks taps on M: rows (j, co), j = 3a + b standing
+// for dy = 1 - a, dz = 1 - b, read from dy staged as [row][plane][co][8 x]
+// with the three planes z-1, z, z+1 in consecutive 256-byte blocks, so the
+// 16 row groups of taps j = 0..7 lie 128 B apart (a uniform stride) and the
+// second K row is three blocks on.  One staged copy per x shift dx keeps the
+// operands 16-byte aligned; per K slice and shift one MMA covers taps 0..7
+// and a second, one block later, taps 1..8 (only its last 16 rows, tap 8,
+// are kept).  Six accumulators of 16 TMEM columns sum over all units of a
+// CTA; the CTA's 27 x 16 x 16 sums go to partial[cta] for the fixed-order
+// reduction.  Every wait is bounded; on a timeout the CTA sets the status
+// flag and writes NaN partial sums.
+constexpr int kWgRows = 16;                           // y rows of a unit
+constexpr int kWgX = 8;                               // x voxels of a unit
+constexpr int kWgXBytes = kWgRows * 256;              // staged x: [row][ci][8]
+constexpr int kWgDyBytes = (kWgRows + 2) * 3 * 256;   // staged dy per shift
+constexpr int kWgSmem = kWgXBytes + 3 * kWgDyBytes + 128;
+constexpr int kWgThreads = 128;
+
+__global__ void __launch_bounds__(kWgThreads)
+k_conv3d_wgrad_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ dy,
+                  int D, int H, int W, float *__restrict__ partial) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  unsigned char *sxs = smem;                  // [row][ci][8 x]
+  unsigned char *sdy = smem + kWgXBytes;      // [dx][row][plane][co][8 x]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nxw = (W + kWgX - 1) / kWgX, nyb = (H + kWgRows - 1) / kWgRows;
+  const long long nunits = (long long)nxw * nyb * D;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(
+                     smem_u32(&tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t xa = smem_u32(sxs), da = smem_u32(sdy);
+  int phase = 0;
+  bool ok = true, any = false;
+  for (long long unit = blockIdx.x; unit < nunits && ok; unit += gridDim.x) {
+    const int xw = (int)(unit % nxw);
+    const long long r0 = unit / nxw;
+    const int yb = (int)(r0 % nyb), z = (int)(r0 / nyb);
+    const int x0 = xw * kWgX, y0 = yb * kWgRows;
+    // x: voxel (row, k) of the unit, 8 channels per item
+    for (int c = tid; c < kWgRows * kWgX * 2; c += blockDim.x) {
+      const int h = c & 1, k = (c >> 1) % kWgX, row = (c >> 1) / kWgX;
+      const int gy = y0 + row, gx = x0 + k;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (gy < H && gx < W)
+        v = *reinterpret_cast<const uint4 *>(x + (((long long)z * H + gy) * W + gx) * kC + h * 8);
+      const unsigned short *e = reinterpret_cast<const unsigned short *>(&v);
+      unsigned short *dst = reinterpret_cast<unsigned short *>(sxs + row * 256) + k;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) dst[(h * 8 + q) * kWgX] = e[q];
+    }
+    // dy: shift s (dx = s - 1), staged row r (y = y0 - 1 + r), plane b
+    // (z - 1 + b), voxel k (x = x0 + k - dx), 8 channels per item
+    for (int c = tid; c < 3 * (kWgRows + 2) * 3 * kWgX * 2; c += blockDim.x) {
+      const int h = c & 1;
+      int rest = c >> 1;
+      const int k = rest % kWgX;
+      rest /= kWgX;
+      const int b = rest % 3;
+      rest /= 3;
+      const int r = rest % (kWgRows + 2), s = rest / (kWgRows + 2);
+      const int gz = z - 1 + b, gy = y0 - 1 + r, gx = x0 + k - (s - 1);
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (gz >= 0 && gz < D && gy >= 0 && gy < H && gx >= 0 && gx < W)
+        v = *reinterpret_cast<const uint4 *>(dy + (((long long)gz * H + gy) * W + gx) * kC + h * 8);
+      const unsigned short *e = reinterpret_cast<const unsigned short *>(&v);
+      unsigned short *dst =
+          reinterpret_cast<unsigned short *>(sdy + s * kWgDyBytes + (r * 3 + b) * 256) + k;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) dst[(h * 8 + q) * kWgX] = e[q];
+    }
+    fence_proxy_async_smem();  // staged by the threads, read by the tensor cores
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+      for (int r = 0; r < kWgRows; r += 2) {
+        const uint64_t bd = tc_desc(xa + (uint32_t)(r * 256), 256, 128);
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+          const uint32_t a0 = da + (uint32_t)(s * kWgDyBytes + r * 3 * 256);
+          const uint32_t acc = (any || r > 0) ? 1u : 0u;
+          tc_mma(tmem + (uint32_t)(2 * s * kC), tc_desc(a0, 768, 128), bd, acc);
+          tc_mma(tmem + (uint32_t)((2 * s + 1) * kC), tc_desc(a0 + 256, 768, 128), bd, acc);
+        }
+      }
+      tc_commit(&bar);
+    }
+    any = true;
+    ok = __syncthreads_and(mbar_wait_bounded(&bar, (uint32_t)phase));  // staging free again
+    phase ^= 1;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (!ok && tid == 0) {
+    atomicExch(&g_conv_status, EFWI_STATUS_TIMEOUT);
+    mbar_wait_bounded(&bar, (uint32_t)(phase ^ 1));  // the MMAs still in flight, bounded
+  }
+  // the CTA's sums: accumulator 2s holds taps j = 0..7 of shift s in rows
+  // 16 j + co, accumulator 2s + 1 tap j = 8 in rows 112..127; column = ci
+  float *out = partial + (long long)blockIdx.x * 27 * kC * kC;
+  const float nan = __int_as_float(0x7fc00000);
+#pragma unroll 1
+  for (int acc = 0; acc < 6; ++acc) {
+    float v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = 0.f;
+    if (any && ok) tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * kC), v);
+    const int row = warp * 32 + lane, co = row & 15;
+    const int j = (acc & 1) ? 8 : row >> 4;
+    if ((acc & 1) && row < 112) continue;
+    const int a = j / 3, b = j % 3, s = acc >> 1;
+    const int t = (2 - b) * 9 + (2 - a) * 3 + s;  // (dz+1)*9 + (dy+1)*3 + (dx+1)
+    float *o = out + ((long long)t * kC + co) * kC;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) o[q] = ok ? v[q] : nan;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem) : "memory");
+}
+
 }  // namespace
 }  // namespace efwi
 
@@ -867,12 +1006,29 @@ extern "C" int efwi_conv3d_forward(const void *x, const void *w, const float *bi
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
+namespace {
+std::atomic<int> g_wgrad_kernel{0};  // 1: tcgen05, 0: mma.sync
+std::atomic<unsigned long long> g_wg_smem_set{0};
+}  // namespace
+
+extern "C" int efwi_conv3d_set_wgrad_kernel(int tcgen05) {
+  g_wgrad_kernel.store(tcgen05 ? 1 : 0);
+  return 0;
+}
+
 extern "C" int efwi_conv3d_wgrad(const void *x, const void *dy, int D, int H, int W,
                                  float *partial, int nparts, float *dw, void *stream) {
   if (!x || !dy || !partial || !dw || D < 1 || H < 1 || W < 1 || nparts < 1) return 1;
   cudaStream_t st = (cudaStream_t)stream;
-  k_conv3d_wgrad<<<nparts, 27 * 32, 0, st>>>((const __nv_bfloat16 *)x, (const __nv_bfloat16 *)dy,
-                                             D, H, W, partial);
+  // the tcgen05 form stages with 16-byte loads; unaligned inputs take mma.sync
+  if (g_wgrad_kernel.load() == 1 && ((uintptr_t)x & 15) == 0 && ((uintptr_t)dy & 15) == 0) {
+    set_smem_once(k_conv3d_wgrad_tc, kWgSmem, g_wg_smem_set);
+    k_conv3d_wgrad_tc<<<nparts, kWgThreads, kWgSmem, st>>>(
+        (const __nv_bfloat16 *)x, (const __nv_bfloat16 *)dy, D, H, W, partial);
+  } else {
+    k_conv3d_wgrad<<<nparts, 27 * 32, 0, st>>>((const __nv_bfloat16 *)x,
+                                               (const __nv_bfloat16 *)dy, D, H, W, partial);
+  }
   const int n = 27 * kC * kC;
   k_reduce_partials<<<(n + 255) / 256, 256, 0, st>>>(partial, nparts, n, dw);
   return cudaGetLastError() == cudaSuccess ? 0 : 2;

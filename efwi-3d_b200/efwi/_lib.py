@@ -105,6 +105,7 @@ _SIGS = {
                                     C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "efwi_conv3d_set_kernel": (C.c_int, [C.c_int]),
     "efwi_conv3d_status": (C.c_int, [C.POINTER(C.c_int), C.c_void_p]),
+    "efwi_conv3d_set_wgrad_kernel": (C.c_int, [C.c_int]),
     "efwi_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "efwi_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong),
                                     C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

@@ -62,6 +62,14 @@ def set_conv_kernel(form: str) -> None:
     lib().efwi_conv3d_set_kernel(CONV_FORMS[form])
 
 
+def set_wgrad_kernel(form: str) -> None:
+    """'tcgen05' (eight taps per MMA, accumulators in tensor memory) or 'mma'
+    (mma.sync, the default) for every later weight-gradient convolution."""
+    if form not in ("tcgen05", "mma"):
+        raise ValueError(f"unknown weight-gradient kernel form {form!r}")
+    lib().efwi_conv3d_set_wgrad_kernel(1 if form == "tcgen05" else 0)
+
+
 def conv3d_status(device=None) -> bool:
     """True when a tcgen05 convolution since the last call gave up waiting for
     its tensor cores (its outputs are then incomplete); clears the flag."""

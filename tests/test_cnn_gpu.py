@@ -73,6 +73,31 @@ def test_tcgen05_form_matches_mma_form_and_torch(shape, form_tc):
         set_conv_kernel(DEFAULT_FORM)
 
 
+@pytest.mark.parametrize("shape", [(1, 1, 1), (3, 17, 9), (6, 7, 41), (5, 40, 24)])
+def test_tcgen05_weight_gradient_matches_mma_and_torch(shape):
+    """The tcgen05 weight gradient (eight taps per MMA) against the mma.sync
+    one and torch's FP32 conv3d_weight of the same BF16 operands, on units
+    (8 x 16 voxels) cut at every edge; 1e-5 rel-L2."""
+    from efwi.cnn import conv3d_status, conv3d_wgrad, set_wgrad_kernel
+    g = torch.Generator(device="cuda").manual_seed(9)
+    x = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
+    dy = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
+    w = torch.zeros(27, 16, 16)
+    ref = torch.nn.grad.conv3d_weight(_ncdhw(x), _torch_w(w).shape, _ncdhw(dy), padding=1)
+    ref = ref.permute(2, 3, 4, 0, 1).reshape(27, 16, 16)
+    try:
+        set_wgrad_kernel("mma")
+        mma = conv3d_wgrad(x, dy)
+        set_wgrad_kernel("tcgen05")
+        tc = conv3d_wgrad(x, dy)
+        torch.cuda.synchronize()
+        assert not conv3d_status()
+    finally:
+        set_wgrad_kernel("mma")
+    assert rel_l2(tc.cpu(), ref.cpu()) < 1e-5
+    assert rel_l2(tc.cpu(), mma.cpu()) < 1e-5
+
+
 def test_input_and_weight_gradients_match_torch():
     from efwi.cnn import conv3d_raw, conv3d_wgrad
     g = torch.Generator(device="cuda").manual_seed(2)
