@@ -590,7 +590,7 @@ def run_cnn(a):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / a.steps
         wgrad[form] = {"ms": ms, "tflops": fl1 / (ms * 1e-3) / 1e12}
-    set_wgrad_kernel("mma")
+    set_wgrad_kernel("tcgen05")
     if conv3d_status():
         raise RuntimeError("a tcgen05 convolution timed out waiting for its tensor cores")
     set_conv_kernel(a.conv_form)
@@ -621,7 +621,7 @@ def run_cnn(a):
                       "peak_bf16_tflops": peak, "peak_hbm_gbs": hbm,
                       "network_form": a.conv_form,
                       "note": "network: forward and input-gradient convolutions in the named "
-                              "form, mma.sync weight gradient; FP32 accumulation"}))
+                              "form, tcgen05 weight gradient; FP32 accumulation"}))
 
 
 def main():

@@ -1007,7 +1007,7 @@ extern "C" int efwi_conv3d_forward(const void *x, const void *w, const float *bi
 }
 
 namespace {
-std::atomic<int> g_wgrad_kernel{0};  // 1: tcgen05, 0: mma.sync
+std::atomic<int> g_wgrad_kernel{1};  // 1: tcgen05, 0: mma.sync
 std::atomic<unsigned long long> g_wg_smem_set{0};
 }  // namespace
 

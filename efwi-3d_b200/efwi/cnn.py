@@ -63,8 +63,9 @@ def set_conv_kernel(form: str) -> None:
 
 
 def set_wgrad_kernel(form: str) -> None:
-    """'tcgen05' (eight taps per MMA, accumulators in tensor memory) or 'mma'
-    (mma.sync, the default) for every later weight-gradient convolution."""
+    """'tcgen05' (eight taps per MMA, accumulators in tensor memory; the
+    default) or 'mma' (mma.sync) for every later weight-gradient
+    convolution."""
     if form not in ("tcgen05", "mma"):
         raise ValueError(f"unknown weight-gradient kernel form {form!r}")
     lib().efwi_conv3d_set_wgrad_kernel(1 if form == "tcgen05" else 0)

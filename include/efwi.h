@@ -291,7 +291,7 @@ int efwi_conv3d_set_kernel(int form);
 int efwi_conv3d_status(int *timed_out, void *stream);
 /* Kernel form of efwi_conv3d_wgrad for this process: 1 = tcgen05.mma (eight
  * taps stacked on the 128 rows of one MMA, K = 16 voxels, accumulators in
- * tensor memory; 16-byte aligned inputs), 0 = mma.sync (the default).  The
+ * tensor memory; 16-byte aligned inputs; the default), 0 = mma.sync.  The
  * same sums up to FP32 rounding order; a bounded wait that ran out sets the
  * efwi_conv3d_status flag and leaves NaN in that CTA's partial sums. */
 int efwi_conv3d_set_wgrad_kernel(int tcgen05);

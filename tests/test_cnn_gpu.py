@@ -93,7 +93,7 @@ def test_tcgen05_weight_gradient_matches_mma_and_torch(shape):
         torch.cuda.synchronize()
         assert not conv3d_status()
     finally:
-        set_wgrad_kernel("mma")
+        set_wgrad_kernel("tcgen05")
     assert rel_l2(tc.cpu(), ref.cpu()) < 1e-5
     assert rel_l2(tc.cpu(), mma.cpu()) < 1e-5
 
