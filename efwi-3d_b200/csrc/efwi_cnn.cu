@@ -747,8 +747,9 @@ k_conv3d_fwd_ws(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *_
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
 }
 // Weight gradient on tcgen05: dW[t][co][ci] = sum_u dy[u - off_t][co] x[u][ci]
-// (u = v + off_t).  A unit is 8 (x) x 16 (y) voxels u at one z; its K = 16
-// slices are two staged rows of 8 voxels.  B = x[u][ci] staged as
+// (u = v + off_t).  A unit is 8 (x) x 16 (y) voxels u on each of up to 8
+// consecutive z planes (the dy planes of one z are reused for the next);
+// its K = 16 slices are two staged rows of 8 voxels.  B = x[u][ci] staged as
 // [row][ci][8 x] (256-byte row blocks: ci halves 128 B apart, the second K
 // row one block on).  A stacks taps on M: rows (j, co), j = 3a + b standing
 // for dy = 1 - a, dz = 1 - b, read from dy staged as [row][plane][co][8 x]
@@ -762,6 +763,7 @@ k_conv3d_fwd_ws(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16 *_
 // reduction.  Every wait is bounded; on a timeout the CTA sets the status
 // flag and writes NaN partial sums.
 constexpr int kWgRows = 16;                           // y rows of a unit
+constexpr int kWgZ = 8;                               // z planes a unit marches
 constexpr int kWgX = 8;                               // x voxels of a unit
 constexpr int kWgXBytes = kWgRows * 256;              // staged x: [row][ci][8]
 constexpr int kWgDyBytes = (kWgRows + 2) * 3 * 256;   // staged dy per shift
@@ -779,7 +781,7 @@ k_conv3d_wgrad_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__re
   unsigned char *sdy = smem + kWgXBytes;      // [dx][row][plane][co][8 x]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nxw = (W + kWgX - 1) / kWgX, nyb = (H + kWgRows - 1) / kWgRows;
-  const long long nunits = (long long)nxw * nyb * D;
+  const long long nunits = (long long)nxw * nyb * ((D + kWgZ - 1) / kWgZ);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(
                      smem_u32(&tmem_slot))
@@ -797,64 +799,83 @@ k_conv3d_wgrad_tc(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__re
   const uint32_t xa = smem_u32(sxs), da = smem_u32(sdy);
   int phase = 0;
   bool ok = true, any = false;
-  for (long long unit = blockIdx.x; unit < nunits && ok; unit += gridDim.x) {
-    const int xw = (int)(unit % nxw);
-    const long long r0 = unit / nxw;
-    const int yb = (int)(r0 % nyb), z = (int)(r0 / nyb);
-    const int x0 = xw * kWgX, y0 = yb * kWgRows;
-    // x: voxel (row, k) of the unit, 8 channels per item
-    for (int c = tid; c < kWgRows * kWgX * 2; c += blockDim.x) {
-      const int h = c & 1, k = (c >> 1) % kWgX, row = (c >> 1) / kWgX;
-      const int gy = y0 + row, gx = x0 + k;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (gy < H && gx < W)
-        v = *reinterpret_cast<const uint4 *>(x + (((long long)z * H + gy) * W + gx) * kC + h * 8);
-      const unsigned short *e = reinterpret_cast<const unsigned short *>(&v);
-      unsigned short *dst = reinterpret_cast<unsigned short *>(sxs + row * 256) + k;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) dst[(h * 8 + q) * kWgX] = e[q];
-    }
-    // dy: shift s (dx = s - 1), staged row r (y = y0 - 1 + r), plane b
-    // (z - 1 + b), voxel k (x = x0 + k - dx), 8 channels per item
-    for (int c = tid; c < 3 * (kWgRows + 2) * 3 * kWgX * 2; c += blockDim.x) {
+  // dy of plane gz into plane slot b of every shift copy (zeros outside)
+  auto stage_dy_plane = [&](int b, int gz, int x0, int y0) {
+    for (int c = tid; c < 3 * (kWgRows + 2) * kWgX * 2; c += blockDim.x) {
       const int h = c & 1;
       int rest = c >> 1;
       const int k = rest % kWgX;
       rest /= kWgX;
-      const int b = rest % 3;
-      rest /= 3;
-      const int r = rest % (kWgRows + 2), s = rest / (kWgRows + 2);
-      const int gz = z - 1 + b, gy = y0 - 1 + r, gx = x0 + k - (s - 1);
+      const int r = rest % (kWgRows + 2), sh = rest / (kWgRows + 2);
+      const int gy = y0 - 1 + r, gx = x0 + k - (sh - 1);
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
       if (gz >= 0 && gz < D && gy >= 0 && gy < H && gx >= 0 && gx < W)
         v = *reinterpret_cast<const uint4 *>(dy + (((long long)gz * H + gy) * W + gx) * kC + h * 8);
       const unsigned short *e = reinterpret_cast<const unsigned short *>(&v);
       unsigned short *dst =
-          reinterpret_cast<unsigned short *>(sdy + s * kWgDyBytes + (r * 3 + b) * 256) + k;
+          reinterpret_cast<unsigned short *>(sdy + sh * kWgDyBytes + (r * 3 + b) * 256) + k;
 #pragma unroll
       for (int q = 0; q < 8; ++q) dst[(h * 8 + q) * kWgX] = e[q];
     }
-    fence_proxy_async_smem();  // staged by the threads, read by the tensor cores
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll 1
-      for (int r = 0; r < kWgRows; r += 2) {
-        const uint64_t bd = tc_desc(xa + (uint32_t)(r * 256), 256, 128);
-#pragma unroll
-        for (int s = 0; s < 3; ++s) {
-          const uint32_t a0 = da + (uint32_t)(s * kWgDyBytes + r * 3 * 256);
-          const uint32_t acc = (any || r > 0) ? 1u : 0u;
-          tc_mma(tmem + (uint32_t)(2 * s * kC), tc_desc(a0, 768, 128), bd, acc);
-          tc_mma(tmem + (uint32_t)((2 * s + 1) * kC), tc_desc(a0 + 256, 768, 128), bd, acc);
+  };
+  for (long long unit = blockIdx.x; unit < nunits && ok; unit += gridDim.x) {
+    const int xw = (int)(unit % nxw);
+    const long long r0 = unit / nxw;
+    const int yb = (int)(r0 % nyb), zc = (int)(r0 / nyb);
+    const int x0 = xw * kWgX, y0 = yb * kWgRows;
+    const int zb = zc * kWgZ, ze = min(zb + kWgZ, D);
+    for (int z = zb; z < ze && ok; ++z) {
+      if (z == zb) {
+        for (int b = 0; b < 3; ++b) stage_dy_plane(b, z - 1 + b, x0, y0);
+      } else {
+        // planes z-1, z of the new window are planes 1, 2 of the last one:
+        // each thread moves its own 16-byte pieces, then plane z+1 arrives
+        for (int c = tid; c < 3 * (kWgRows + 2) * 16; c += blockDim.x) {
+          const int piece = c & 15, rs = c >> 4;  // rs = shift * (rows) + row
+          uint4 *blk = reinterpret_cast<uint4 *>(sdy + (rs / (kWgRows + 2)) * kWgDyBytes +
+                                                 (rs % (kWgRows + 2)) * 3 * 256);
+          const uint4 p1 = blk[16 + piece], p2 = blk[32 + piece];
+          blk[piece] = p1;
+          blk[16 + piece] = p2;
         }
+        __syncthreads();  // plane slot 2 is rewritten below by other threads
+        stage_dy_plane(2, z + 1, x0, y0);
       }
-      tc_commit(&bar);
+      // x: voxel (row, k) of plane z, 8 channels per item
+      for (int c = tid; c < kWgRows * kWgX * 2; c += blockDim.x) {
+        const int h = c & 1, k = (c >> 1) % kWgX, row = (c >> 1) / kWgX;
+        const int gy = y0 + row, gx = x0 + k;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (gy < H && gx < W)
+          v = *reinterpret_cast<const uint4 *>(x + (((long long)z * H + gy) * W + gx) * kC + h * 8);
+        const unsigned short *e = reinterpret_cast<const unsigned short *>(&v);
+        unsigned short *dst = reinterpret_cast<unsigned short *>(sxs + row * 256) + k;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) dst[(h * 8 + q) * kWgX] = e[q];
+      }
+      fence_proxy_async_smem();  // staged by the threads, read by the tensor cores
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+        for (int r = 0; r < kWgRows; r += 2) {
+          const uint64_t bd = tc_desc(xa + (uint32_t)(r * 256), 256, 128);
+#pragma unroll
+          for (int sh = 0; sh < 3; ++sh) {
+            const uint32_t a0 = da + (uint32_t)(sh * kWgDyBytes + r * 3 * 256);
+            const uint32_t acc = (any || r > 0) ? 1u : 0u;
+            tc_mma(tmem + (uint32_t)(2 * sh * kC), tc_desc(a0, 768, 128), bd, acc);
+            tc_mma(tmem + (uint32_t)((2 * sh + 1) * kC), tc_desc(a0 + 256, 768, 128), bd, acc);
+          }
+        }
+        tc_commit(&bar);
+      }
+      any = true;
+      // the staged planes are read by the MMAs: wait before changing them
+      ok = __syncthreads_and(mbar_wait_bounded(&bar, (uint32_t)phase));
+      phase ^= 1;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
-    any = true;
-    ok = __syncthreads_and(mbar_wait_bounded(&bar, (uint32_t)phase));  // staging free again
-    phase ^= 1;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
   if (!ok && tid == 0) {
     atomicExch(&g_conv_status, EFWI_STATUS_TIMEOUT);
