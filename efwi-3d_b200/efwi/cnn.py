@@ -83,7 +83,7 @@ def conv3d_status(device=None) -> bool:
     return bool(flag.value)
 
 
-def conv3d_wgrad(x: torch.Tensor, dy: torch.Tensor, nparts: int = 296) -> torch.Tensor:
+def conv3d_wgrad(x: torch.Tensor, dy: torch.Tensor, nparts: int = 592) -> torch.Tensor:
     """dW[t][co][ci] = sum_v dy[v][co] x[v + off_t][ci] (f32)."""
     D, H, W = x.shape[:3]
     partial = torch.empty(nparts * 27 * C16 * C16, device=x.device, dtype=torch.float32)
