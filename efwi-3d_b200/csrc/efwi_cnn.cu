@@ -7,19 +7,25 @@
 //   activations  [D][H][W][16] bf16 (channels last: one voxel = 32 bytes)
 //   weights      [27][16 co][16 ci] bf16, tap t = (dz+1)*9 + (dy+1)*3 + (dx+1)
 //   bias         [16] f32
-// The convolution is an implicit GEMM: per output voxel row of 16
-// consecutive x, one warp accumulates sum over taps t and input channels of
-// X[v + off_t][ci] W[t][co][ci] with mma.m16n8k16 (bf16 in, f32 accumulate):
-// A = 16 voxels x 16 input channels of one tap (ldmatrix from the CTA's
-// staged input tile), B = 16 input channels x 8 output channels, two
-// n-tiles.  Voxels outside the volume read as zero.
+// Voxels outside the volume read as zero.  With W'[t][a][b] = W[26-t][b][a]
+// the forward convolution also computes the gradient of the input (the
+// transposed convolution).
 //
-//   k_conv3d_fwd     y = act(conv(x, W) + b), stored as bf16 and/or f32.
-//                    With W'[t][a][b] = W[26-t][b][a] it also computes the
-//                    gradient of the input (the transposed convolution).
-//   k_conv3d_wgrad   dW[t][co][ci] = sum_v dy[v][co] x[v + off_t][ci]: one
-//                    warp per tap, K = voxels (16 per mma), per-CTA partial
-//                    sums reduced in a fixed order by k_reduce_partials.
+// Kernels (efwi_conv3d_set_kernel / efwi_conv3d_set_wgrad_kernel choose):
+//   k_conv3d_fwd_tc2  forward on tcgen05.mma (the default): per tile of
+//                     128 voxels one MMA per tap, accumulator in tensor
+//                     memory, input tiles staged by bulk tensor copies
+//   k_conv3d_fwd_ws   the same, warp-specialised (copy + MMA warp, four
+//                     epilogue warps)
+//   k_conv3d_fwd_tc   the same MMAs, tiles staged by plain loads
+//   k_conv3d_fwd      forward on mma.sync.m16n8k16: per output row of 16
+//                     voxels one warp, A fragments by ldmatrix
+//   k_conv3d_wgrad_tc dW[t][co][ci] = sum_u dy[u - off_t][co] x[u][ci] on
+//                     tcgen05.mma (the default): eight taps stacked on the
+//                     MMA's rows, K = voxels
+//   k_conv3d_wgrad    the same on mma.sync: one warp per tap
+// Both weight gradients leave per-CTA partial sums that k_reduce_partials
+// adds in a fixed order.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
